@@ -1,0 +1,142 @@
+/*
+ * sumcheck_b200.h -- C ABI of the B200 SumCheck prover (libsumcheck_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes; no CUDA, torch or C++ types. Every call
+ * returns SC_OK (0) or an SC_ERR_* code; sc_last_error() gives the message of the
+ * calling thread's last failure. Device work runs on the stream given to sc_ctx_create.
+ *
+ * The reference (snarang181/sumcheck-triton) exposes this path two ways, and nothing
+ * here is a binding of its code: its Python API `zkduel.sumcheck(eval_tables, q,
+ * expression, challenges, num_rounds, bit_width, backend)` (src/zkduel/api.py:26-64)
+ * and its CUDA executable's round loop (cuda/src/field_sumcheck.cu:1012-1088, CLI
+ * :1091-1176). Each entry point below names the reference interface it replaces.
+ *
+ * Data formats
+ *   field element  L little-endian u32 limbs, L in {1, 2, 4, 8}; "Montgomery" means the
+ *                  limbs of x * 2^(32 L) mod p, always fully reduced (< p).
+ *   tables         limb-planar device memory: table k, limb l is the u32 plane
+ *                  tables[(k * L + l) * 2^n + i], i < 2^n. Device pointer, 16-byte aligned.
+ *   expression     sum of terms coeff * prod(tables): term i has term_lens[i] factors
+ *                  flat[term_offsets[i] ...], each a table index < num_vars.
+ */
+#ifndef SUMCHECK_B200_H
+#define SUMCHECK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SC_OK 0
+#define SC_ERR_INVALID 1        /* bad argument (sizes, alignment, NULL, ranges)        */
+#define SC_ERR_UNSAFE_MODULUS 2 /* modulus outside the Montgomery product's exactness   */
+#define SC_ERR_CUDA 3           /* a CUDA runtime call failed                            */
+#define SC_ERR_UNSUPPORTED 4    /* outside the compiled limits (degree, tables, terms)  */
+#define SC_ERR_DEVICE 5         /* the device reported an error status                  */
+#define SC_ERR_NOMEM 6          /* device or host allocation failed                     */
+
+#define SC_CHALLENGE_SHA3 0     /* r_j = SHA3 transcript rule (field_sumcheck.cu:857-907) */
+#define SC_CHALLENGE_FIXED 1    /* r_j = 1 (field_sumcheck.cu:1058)                       */
+#define SC_CHALLENGE_EXPLICIT 2 /* r_j given by the caller (api.py:26-35 `challenges`)    */
+
+#define SC_TABLE_UNIFORM 0      /* uniform in [0, p): counter-based SplitMix64 + rejection */
+#define SC_TABLE_BERNOULLI 1    /* 0/1 selectors                                           */
+#define SC_TABLE_ARITH 2        /* SC_TABLE_ARITH + v: the reference's fill of table v     */
+                                /* (seed + 7919 (v+1) + 104729 (off+1)) mod p,             */
+                                /* field_sumcheck.cu:123-128, :593-611                     */
+
+#define SC_MAX_LIMBS 8
+#define SC_MAX_DEGREE 7         /* 8 interpolation points, field_sumcheck.cu:29 */
+#define SC_MAX_VARS 32
+#define SC_MAX_TERMS 32
+#define SC_MAX_FACTORS 128      /* total factors over all terms */
+#define SC_MAX_ROUNDS 40
+
+typedef struct sc_ctx sc_ctx;
+typedef struct sc_field sc_field;
+typedef struct sc_expr sc_expr;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int sc_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* sc_last_error(void);
+
+/* A prover context on `device`, issuing all work on `stream` (a cudaStream_t; NULL for
+ * the legacy default stream). Owns the scratch buffers (fold ping-pong, block partials,
+ * proof state), grown on demand. One context per host thread.
+ * Replaces: the CUDA executable's per-run setup (field_sumcheck.cu:1178-1225). */
+int sc_ctx_create(int device, void* stream, sc_ctx** out);
+int sc_ctx_destroy(sc_ctx* ctx);
+/* Waits for all work of the context's stream. */
+int sc_ctx_synchronize(sc_ctx* ctx);
+
+/* A field of modulus p (L limbs) with nprime = -p^-1 mod 2^32. Rejects, with
+ * SC_ERR_UNSAFE_MODULUS, the moduli the reference's guard rejects: even or < 3, wrong
+ * nprime, or outside (2p-1) + (p-1)(2^32-1) < 2^(32(L+1)).
+ * Replaces: zkduel.fields.FieldSpec / check_montgomery_modulus (src/zkduel/fields.py:190-255)
+ * and the executable's FIELDS table (field_sumcheck.cu:39-121). */
+int sc_field_init(int limbs, const uint32_t* modulus, uint32_t nprime, sc_field** out);
+int sc_field_destroy(sc_field* field);
+
+/* A constraint expression. coeffs[i] is term i's integer coefficient; if coeff_limbs is
+ * not NULL it overrides coeffs with non-negative 8-limb values (num_terms x 8 u32), for
+ * coefficients beyond int64 (the caller reduces them mod p).
+ * Replaces: encode_expression_with_coeffs (src/zkduel/_expr.py:87-110) and the
+ * executable's per-workload templates (field_sumcheck.cu:389-590). */
+int sc_expr_compile(int num_vars, int num_terms, const int64_t* coeffs,
+                    const uint32_t* coeff_limbs, const int32_t* term_lens,
+                    const int32_t* term_offsets, const int32_t* flat, sc_expr** out);
+int sc_expr_destroy(sc_expr* expr);
+int sc_expr_degree(const sc_expr* expr);
+int sc_expr_num_vars(const sc_expr* expr);
+
+/* Fills num_tables tables of 2^num_rounds entries (Montgomery, limb-planar) at tables_dev.
+ * kinds[k] is SC_TABLE_UNIFORM, SC_TABLE_BERNOULLI or SC_TABLE_ARITH + v.
+ * Replaces: fill_tables_kernel (field_sumcheck.cu:593-611) and the Triton _make_tables
+ * (benchmarks/field_sweep/triton_sweep.py:425-452). Asynchronous. */
+int sc_tables_generate(sc_ctx* ctx, const sc_field* field, int num_tables, int num_rounds,
+                       const int32_t* kinds, uint64_t seed, uint32_t* tables_dev);
+
+/* In-place conversion of num_tables x L planes of `entries` values between canonical
+ * form (< p) and Montgomery form. Asynchronous.
+ * Replaces: the Triton backend's host Montgomery encode/decode
+ * (src/zkduel/triton_backend/u256_sumcheck.py:99-109). */
+int sc_tables_to_mont(sc_ctx* ctx, const sc_field* field, uint32_t* tables_dev,
+                      uint64_t entries, int num_tables);
+int sc_tables_from_mont(sc_ctx* ctx, const sc_field* field, uint32_t* tables_dev,
+                        uint64_t entries, int num_tables);
+
+/* Element-wise field arithmetic on device arrays of count elements (element-major, L words
+ * each, values < p): op 0 = Montgomery product a b R^-1, 1 = a + b, 2 = a - b (mod p).
+ * Exposes the prover's own device arithmetic for checking against big integers.
+ * Replaces: the Triton backend's elementwise uint256 kernels
+ * (src/zkduel/triton_backend/uint256.py:1149-1313). Asynchronous. */
+int sc_field_apply(sc_ctx* ctx, const sc_field* field, int op, const uint32_t* a_dev,
+                   const uint32_t* b_dev, uint32_t* out_dev, uint64_t count);
+
+/* One SumCheck proof over num_rounds variables: num_rounds launches, no host round trip,
+ * then one copy of the results to the host (the call returns when they are there).
+ *   tables_dev           num_vars tables of 2^num_rounds entries, Montgomery, limb-planar;
+ *                        read only.
+ *   challenge_mode       SC_CHALLENGE_*; explicit_challenges (host, num_rounds x L,
+ *                        Montgomery) is read only in SC_CHALLENGE_EXPLICIT mode.
+ * Outputs (host, Montgomery limbs; any may be NULL):
+ *   out_round_polys      num_rounds x (degree + 1) x L: g_j(0..degree)
+ *   out_challenges       num_rounds x L: r_j (r_{n-1} is the final-point challenge)
+ *   out_finals           (1 + num_vars) x L: g_{n-1}(r_{n-1}), then f_k(r_0..r_{n-1})
+ *   out_claim0           L: g_0(0) + g_0(1), the sum over the hypercube
+ *   out_checksum         sum over rounds and points of sum_i (i + 1) limb_i
+ * Replaces: zkduel.sumcheck (src/zkduel/api.py:26-64) and run_once
+ * (field_sumcheck.cu:1012-1088). */
+int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,
+             const uint32_t* tables_dev, int challenge_mode, const uint32_t* explicit_challenges,
+             uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
+             uint32_t* out_claim0, uint64_t* out_checksum);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUMCHECK_B200_H */

@@ -1,0 +1,625 @@
+// libsumcheck_b200: the C ABI declared in include/sumcheck_b200.h.
+//
+// Host side of the prover: field and expression set-up, the scratch-owning context,
+// table generation and the per-proof launch sequence. The reference drives its CUDA
+// kernels from a CLI loop with a blocking device-to-host copy per interpolation point
+// (cuda/src/field_sumcheck.cu:1012-1088); here a proof is num_rounds launches of one
+// fused round kernel on the caller's stream and a single copy of the results at the end.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sumcheck_b200.h"
+#include "host_field.h"
+#include "prover.cuh"
+#include "tables.cuh"
+
+using namespace sc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define SC_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return fail(SC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kBlock = 256;
+constexpr int kMaxDynSmem = 200 * 1024;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct sc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  DevBuf fold_a, fold_b, partials, state;
+  uint32_t* host_state = nullptr;  // pinned staging of the proof state
+  size_t host_state_bytes = 0;
+};
+
+struct sc_field {
+  HostField hf;
+  FieldConsts consts;        // host copy
+  FieldConsts* dev = nullptr;
+  int device = -1;
+  bool has_inverses = true;
+};
+
+struct sc_expr {
+  int num_vars = 0, num_terms = 0, degree = 0;
+  std::vector<int64_t> coeffs;
+  std::vector<uint32_t> coeff_limbs;  // num_terms x 8 when given
+  std::vector<int32_t> lens, offs, flat;
+};
+
+namespace {
+
+int ensure(sc_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (bytes <= b.bytes) return SC_OK;
+  if (b.p) {
+    SC_CUDA(cudaStreamSynchronize(ctx->stream));
+    SC_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    return fail(SC_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return SC_OK;
+}
+
+template <int L>
+int set_kernel_attrs() {
+  SC_CUDA(cudaFuncSetAttribute(round_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+  return SC_OK;
+}
+
+// Montgomery image of a small non-negative integer.
+void mont_small(const HostField& hf, const uint32_t* r2, uint64_t v, uint32_t* out) {
+  uint32_t w[2] = {static_cast<uint32_t>(v), static_cast<uint32_t>(v >> 32)};
+  uint32_t red[8];
+  hf.reduce(w, 2, red);
+  hf.mul(red, r2, out);
+}
+
+void mont_pow(const HostField& hf, const uint32_t* base, const uint32_t* e, const uint32_t* one,
+              uint32_t* out) {
+  uint32_t acc[8];
+  std::memcpy(acc, one, 32);
+  for (int w = hf.L - 1; w >= 0; --w)
+    for (int b = 31; b >= 0; --b) {
+      hf.mul(acc, acc, acc);
+      if ((e[w] >> b) & 1u) hf.mul(acc, base, acc);
+    }
+  std::memcpy(out, acc, 4 * hf.L);
+}
+
+// Checks the CIOS exactness bound: (p - 1) 2^32 + p < 2^(32 (L + 1)).
+bool cios_bound_holds(const HostField& hf) {
+  const int L = hf.L;
+  uint32_t x[10] = {0};
+  uint32_t pm1[8];
+  std::memcpy(pm1, hf.p, 4 * L);
+  pm1[0] -= 1;  // p odd, so no borrow
+  for (int i = 0; i < L; ++i) x[i + 1] = pm1[i];
+  uint64_t c = 0;
+  for (int i = 0; i < L + 2; ++i) {
+    uint64_t s = static_cast<uint64_t>(x[i]) + (i < L ? hf.p[i] : 0u) + c;
+    x[i] = static_cast<uint32_t>(s);
+    c = s >> 32;
+  }
+  return x[L + 1] == 0 && c == 0;
+}
+
+template <int L>
+void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
+  std::memset(&E, 0, sizeof(E));
+  E.num_vars = ex.num_vars;
+  E.num_terms = ex.num_terms;
+  E.degree = ex.degree;
+  const HostField& hf = f.hf;
+  const int mul_cost = 4 * L * L + 8 * L, add_cost = 3 * L + 3;
+  for (int i = 0; i < ex.num_terms; ++i) {
+    E.term_len[i] = static_cast<uint8_t>(ex.lens[i]);
+    E.term_off[i] = static_cast<uint8_t>(ex.offs[i]);
+    bool use_mont = !ex.coeff_limbs.empty();
+    const int64_t c = ex.coeffs[i];
+    if (!use_mont) {
+      if (c == 1) {
+        E.coeff_kind[i] = kCoeffPlus;
+      } else if (c == -1) {
+        E.coeff_kind[i] = kCoeffMinus;
+      } else if (c > -(int64_t{1} << 31) && c < (int64_t{1} << 31)) {
+        const uint64_t m = c < 0 ? static_cast<uint64_t>(-c) : static_cast<uint64_t>(c);
+        const int bits = m ? 64 - __builtin_clzll(m) : 0;
+        const int chain = (bits > 0 ? bits - 1 : 0) + (m ? __builtin_popcountll(m) - 1 : 0) + (c < 0);
+        if (chain * add_cost <= mul_cost) {
+          E.coeff_kind[i] = kCoeffSmall;
+          E.coeff_small[i] = static_cast<int32_t>(c);
+        } else {
+          use_mont = true;
+        }
+      } else {
+        use_mont = true;
+      }
+    }
+    if (use_mont) {
+      E.coeff_kind[i] = kCoeffMont;
+      uint32_t red[8];
+      if (!ex.coeff_limbs.empty()) {
+        hf.reduce(&ex.coeff_limbs[8 * i], 8, red);
+      } else {
+        const uint64_t m = c < 0 ? static_cast<uint64_t>(-(c + 1)) + 1u : static_cast<uint64_t>(c);
+        uint32_t w[2] = {static_cast<uint32_t>(m), static_cast<uint32_t>(m >> 32)};
+        hf.reduce(w, 2, red);
+        if (c < 0) hf.neg(red, red);
+      }
+      uint32_t mont[8];
+      hf.mul(red, f.consts.r2, mont);
+      for (int l = 0; l < L; ++l) E.coeff_mont[i][l] = mont[l];
+    }
+  }
+  for (size_t i = 0; i < ex.flat.size(); ++i) E.flat[i] = static_cast<uint8_t>(ex.flat[i]);
+}
+
+struct StateOffsets {
+  size_t counter, status, checksum, polys, chals, finals, claim0, total_words;
+};
+
+StateOffsets state_offsets(int n, int K, int L) {
+  StateOffsets o;
+  o.counter = 0;
+  o.status = 1;
+  o.checksum = 2;  // u64 at word 2 (8-byte aligned)
+  o.polys = 4;
+  o.chals = o.polys + static_cast<size_t>(n) * kMaxPoints * L;
+  o.finals = o.chals + static_cast<size_t>(n) * L;
+  o.claim0 = o.finals + static_cast<size_t>(1 + K) * L;
+  o.total_words = o.claim0 + L;
+  return o;
+}
+
+template <int L>
+int prove_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables,
+               int mode, const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch,
+               uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum) {
+  const int K = ex->num_vars, d = ex->degree;
+  const uint64_t N = uint64_t{1} << n;
+  // scratch
+  const size_t fold_a_words = n >= 2 ? static_cast<size_t>(K) * L * (N / 2) : 0;
+  const size_t fold_b_words = n >= 3 ? static_cast<size_t>(K) * L * (N / 4) : 0;
+  int rc;
+  if ((rc = ensure(ctx, ctx->fold_a, fold_a_words * 4))) return rc;
+  if ((rc = ensure(ctx, ctx->fold_b, fold_b_words * 4))) return rc;
+  const StateOffsets so = state_offsets(n, K, L);
+  if ((rc = ensure(ctx, ctx->state, so.total_words * 4))) return rc;
+
+  int threads = kBlock;
+  const int per_thread = round_smem_words_per_thread(K, L) * 4;
+  while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
+  const size_t smem = static_cast<size_t>(threads) * per_thread;
+  int blocks_per_sm = 0;
+  SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, round_kernel<L>, threads, smem));
+  if (blocks_per_sm < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K, L);
+  const uint64_t grid_max = static_cast<uint64_t>(blocks_per_sm) * ctx->sm_count;
+  if ((rc = ensure(ctx, ctx->partials, grid_max * kMaxPoints * L * 4))) return rc;
+
+  ExprDev E;
+  build_expr_dev<L>(*ex, *f, E);
+  FieldParams<L> F;
+  for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
+  F.np = f->hf.np;
+
+  uint32_t* st = static_cast<uint32_t*>(ctx->state.p);
+  SC_CUDA(cudaMemsetAsync(st, 0, so.total_words * 4, ctx->stream));
+  if (mode == SC_CHALLENGE_EXPLICIT)
+    SC_CUDA(cudaMemcpyAsync(st + so.chals, explicit_ch, static_cast<size_t>(n) * L * 4,
+                            cudaMemcpyHostToDevice, ctx->stream));
+
+  RoundArgs A;
+  A.num_rounds = n;
+  A.mode = mode;
+  A.partials = static_cast<uint32_t*>(ctx->partials.p);
+  A.fc = f->dev;
+  A.st.counter = st + so.counter;
+  A.st.status = st + so.status;
+  A.st.checksum = reinterpret_cast<uint64_t*>(st + so.checksum);
+  A.st.polys = st + so.polys;
+  A.st.chals = st + so.chals;
+  A.st.finals = st + so.finals;
+  A.st.claim0 = st + so.claim0;
+
+  const uint32_t* prev = tables;  // T_{j-1} (or T_0)
+  for (int j = 0; j < n; ++j) {
+    A.round = j;
+    A.pairs = N >> (j + 1);
+    if (j == 0) {
+      A.fold = 0;
+      A.src = tables;
+      A.dst = nullptr;
+      A.src_len = N;
+    } else {
+      A.fold = 1;
+      A.src = prev;
+      A.src_len = N >> (j - 1);
+      A.dst = static_cast<uint32_t*>((j & 1) ? ctx->fold_a.p : ctx->fold_b.p);
+      prev = A.dst;
+    }
+    const uint64_t want = (A.pairs + threads - 1) / threads;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
+    round_kernel<L><<<grid, threads, smem, ctx->stream>>>(A, E, F);
+    SC_CUDA(cudaGetLastError());
+  }
+  // results
+  if (ctx->host_state_bytes < so.total_words * 4) {
+    if (ctx->host_state) cudaFreeHost(ctx->host_state);
+    ctx->host_state = nullptr;
+    ctx->host_state_bytes = 0;
+    SC_CUDA(cudaMallocHost(&ctx->host_state, so.total_words * 4));
+    ctx->host_state_bytes = so.total_words * 4;
+  }
+  SC_CUDA(cudaMemcpyAsync(ctx->host_state, st, so.total_words * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  SC_CUDA(cudaStreamSynchronize(ctx->stream));
+  const uint32_t* hs = ctx->host_state;
+  if (hs[so.status]) return fail(SC_ERR_DEVICE, "device status %u", hs[so.status]);
+  if (out_polys)
+    for (int j = 0; j < n; ++j)
+      std::memcpy(out_polys + static_cast<size_t>(j) * (d + 1) * L, hs + so.polys + static_cast<size_t>(j) * kMaxPoints * L,
+                  static_cast<size_t>(d + 1) * L * 4);
+  if (out_ch) std::memcpy(out_ch, hs + so.chals, static_cast<size_t>(n) * L * 4);
+  if (out_finals) std::memcpy(out_finals, hs + so.finals, static_cast<size_t>(1 + K) * L * 4);
+  if (out_claim0) std::memcpy(out_claim0, hs + so.claim0, L * 4);
+  if (out_checksum) std::memcpy(out_checksum, hs + so.checksum, 8);
+  return SC_OK;
+}
+
+template <int L>
+int generate_impl(sc_ctx* ctx, const sc_field* f, int num_tables, int n, const int32_t* kinds,
+                  uint64_t seed, uint32_t* tables) {
+  TableGenArgs G;
+  std::memset(&G, 0, sizeof(G));
+  G.num_tables = num_tables;
+  G.entries = uint64_t{1} << n;
+  G.seed = seed;
+  for (int k = 0; k < num_tables; ++k) G.kinds[k] = kinds[k];
+  const HostField& hf = f->hf;
+  int bits = 0;
+  for (int l = L - 1; l >= 0 && !bits; --l)
+    if (hf.p[l]) bits = 32 * l + (32 - __builtin_clz(hf.p[l]));
+  for (int l = 0; l < L; ++l) {
+    const int lo = 32 * l;
+    G.mask[l] = bits >= lo + 32 ? 0xFFFFFFFFu : (bits <= lo ? 0u : ((1u << (bits - lo)) - 1u));
+  }
+  bool fits64 = true;
+  for (int l = 2; l < L; ++l) fits64 = fits64 && hf.p[l] == 0;
+  G.p_u64 = fits64 ? (static_cast<uint64_t>(L > 1 ? hf.p[1] : 0) << 32) | hf.p[0] : 0;
+  for (int l = 0; l < L; ++l) G.r2[l] = f->consts.r2[l];
+  FieldParams<L> F;
+  for (int l = 0; l < L; ++l) F.p[l] = hf.p[l];
+  F.np = hf.np;
+  const uint64_t total = G.entries * num_tables;
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, uint64_t{1} << 30));
+  generate_tables_kernel<L><<<grid, 256, 0, ctx->stream>>>(G, F, tables);
+  SC_CUDA(cudaGetLastError());
+  return SC_OK;
+}
+
+template <int L>
+int convert_impl(sc_ctx* ctx, const sc_field* f, uint32_t* tables, uint64_t entries, int num_tables, bool to_mont) {
+  FieldParams<L> F;
+  for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
+  F.np = f->hf.np;
+  Fe<L> factor;
+  for (int l = 0; l < L; ++l) factor.w[l] = to_mont ? f->consts.r2[l] : (l == 0 ? 1u : 0u);
+  const uint64_t total = entries * num_tables;
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, uint64_t{1} << 30));
+  convert_tables_kernel<L><<<grid, 256, 0, ctx->stream>>>(tables, entries, num_tables, factor, F);
+  SC_CUDA(cudaGetLastError());
+  return SC_OK;
+}
+
+template <int L>
+int apply_impl(sc_ctx* ctx, const sc_field* f, int op, const uint32_t* a, const uint32_t* b, uint32_t* out,
+               uint64_t count) {
+  FieldParams<L> F;
+  for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
+  F.np = f->hf.np;
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((count + 255) / 256, uint64_t{1} << 30));
+  field_apply_kernel<L><<<grid, 256, 0, ctx->stream>>>(op, a, b, out, count, F);
+  SC_CUDA(cudaGetLastError());
+  return SC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sc_version(void) { return 100; }
+
+const char* sc_last_error(void) { return g_err.c_str(); }
+
+int sc_ctx_create(int device, void* stream, sc_ctx** out) {
+  if (!out) return fail(SC_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  SC_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(SC_ERR_INVALID, "device %d out of range (%d devices)", device, count);
+  SC_CUDA(cudaSetDevice(device));
+  sc_ctx* c = new (std::nothrow) sc_ctx();
+  if (!c) return fail(SC_ERR_NOMEM, "host allocation failed");
+  c->device = device;
+  c->stream = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(SC_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
+  }
+  int rc;
+  if ((rc = set_kernel_attrs<1>()) || (rc = set_kernel_attrs<2>()) || (rc = set_kernel_attrs<4>()) ||
+      (rc = set_kernel_attrs<8>())) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return SC_OK;
+}
+
+int sc_ctx_destroy(sc_ctx* ctx) {
+  if (!ctx) return SC_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (DevBuf* b : {&ctx->fold_a, &ctx->fold_b, &ctx->partials, &ctx->state})
+    if (b->p) cudaFree(b->p);
+  if (ctx->host_state) cudaFreeHost(ctx->host_state);
+  delete ctx;
+  return SC_OK;
+}
+
+int sc_ctx_synchronize(sc_ctx* ctx) {
+  if (!ctx) return fail(SC_ERR_INVALID, "ctx is NULL");
+  SC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return SC_OK;
+}
+
+int sc_field_init(int limbs, const uint32_t* modulus, uint32_t nprime, sc_field** out) {
+  if (!out || !modulus) return fail(SC_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (limbs != 1 && limbs != 2 && limbs != 4 && limbs != 8)
+    return fail(SC_ERR_UNSUPPORTED, "limbs must be 1, 2, 4 or 8, got %d", limbs);
+  sc_field* f = new (std::nothrow) sc_field();
+  if (!f) return fail(SC_ERR_NOMEM, "host allocation failed");
+  HostField& hf = f->hf;
+  hf.L = limbs;
+  std::memcpy(hf.p, modulus, 4 * limbs);
+  hf.np = nprime;
+  bool big = false;
+  for (int l = 1; l < limbs; ++l) big = big || hf.p[l];
+  if (!(hf.p[0] & 1u) || (!big && hf.p[0] < 3)) {
+    delete f;
+    return fail(SC_ERR_UNSAFE_MODULUS, "Montgomery arithmetic needs an odd modulus > 2");
+  }
+  uint32_t inv = 1;  // p^-1 mod 2^32 by Newton iteration
+  for (int i = 0; i < 5; ++i) inv *= 2u - hf.p[0] * inv;
+  if (nprime != 0u - inv) {
+    delete f;
+    return fail(SC_ERR_UNSAFE_MODULUS, "nprime %#x != -p^-1 mod 2^32 = %#x", nprime, 0u - inv);
+  }
+  if (!cios_bound_holds(hf)) {
+    delete f;
+    return fail(SC_ERR_UNSAFE_MODULUS,
+                "the device Montgomery routine does not support this modulus; it is valid only "
+                "when (2p-1) + (p-1)(2^32-1) < 2^(32(L+1))");
+  }
+  FieldConsts& C = f->consts;
+  std::memset(&C, 0, sizeof(C));
+  std::memcpy(C.p, hf.p, 4 * limbs);
+  C.np = nprime;
+  C.limbs = limbs;
+  C.p_small = big ? 0u : hf.p[0];
+  // R mod p, R^2 mod p, R^2 2^(32 i) mod p by doubling from 1
+  uint32_t x[8] = {0};
+  x[0] = 1;
+  for (int i = 0; i < 32 * limbs; ++i) hf.dbl(x, x);
+  std::memcpy(C.one, x, 4 * limbs);
+  for (int i = 0; i < 32 * limbs; ++i) hf.dbl(x, x);
+  std::memcpy(C.r2, x, 4 * limbs);
+  for (int w = 0; w < 8; ++w) {
+    std::memcpy(C.kdig[w], x, 4 * limbs);
+    for (int i = 0; i < 32; ++i) hf.dbl(x, x);
+  }
+  for (int t = 0; t < kMaxPoints; ++t) mont_small(hf, C.r2, static_cast<uint64_t>(t), C.pts[t]);
+  // Lagrange weights 1 / prod_{s != t} (t - s) (Fermat inverse; verified, p must be prime)
+  uint32_t pm2[8];
+  std::memcpy(pm2, hf.p, 32);
+  pm2[0] -= 2;  // p odd and > 2: no borrow unless p[0] < 2, handled below
+  if (hf.p[0] < 2) {
+    uint32_t two[8] = {2};
+    hf.sub_raw(hf.p, two, pm2);
+  }
+  for (int d = 0; d < kMaxPoints; ++d)
+    for (int t = 0; t <= d; ++t) {
+      int64_t den = 1;
+      for (int s = 0; s <= d; ++s)
+        if (s != t) den *= (t - s);
+      uint32_t dm[8];
+      mont_small(hf, C.r2, static_cast<uint64_t>(den < 0 ? -den : den), dm);
+      if (den < 0) hf.neg(dm, dm);
+      uint32_t inv_m[8], chk[8];
+      mont_pow(hf, dm, pm2, C.one, inv_m);
+      hf.mul(inv_m, dm, chk);
+      if (std::memcmp(chk, C.one, 4 * limbs) != 0) f->has_inverses = false;
+      std::memcpy(C.lag[d][t], inv_m, 4 * limbs);
+    }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaMalloc(&f->dev, sizeof(FieldConsts));
+  if (e == cudaSuccess) e = cudaMemcpy(f->dev, &C, sizeof(FieldConsts), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (f->dev) cudaFree(f->dev);
+    delete f;
+    return fail(SC_ERR_CUDA, "field constants upload: %s", cudaGetErrorString(e));
+  }
+  f->device = dev;
+  *out = f;
+  return SC_OK;
+}
+
+int sc_field_destroy(sc_field* field) {
+  if (!field) return SC_OK;
+  if (field->dev) cudaFree(field->dev);
+  delete field;
+  return SC_OK;
+}
+
+int sc_expr_compile(int num_vars, int num_terms, const int64_t* coeffs, const uint32_t* coeff_limbs,
+                    const int32_t* term_lens, const int32_t* term_offsets, const int32_t* flat,
+                    sc_expr** out) {
+  if (!out || !term_lens || !term_offsets || !flat || (!coeffs && !coeff_limbs))
+    return fail(SC_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (num_vars < 1 || num_vars > kMaxVars) return fail(SC_ERR_UNSUPPORTED, "num_vars %d outside 1..%d", num_vars, kMaxVars);
+  if (num_terms < 1 || num_terms > kMaxTerms) return fail(SC_ERR_UNSUPPORTED, "num_terms %d outside 1..%d", num_terms, kMaxTerms);
+  sc_expr* ex = new (std::nothrow) sc_expr();
+  if (!ex) return fail(SC_ERR_NOMEM, "host allocation failed");
+  ex->num_vars = num_vars;
+  ex->num_terms = num_terms;
+  int total = 0, degree = 0;
+  for (int i = 0; i < num_terms; ++i) {
+    if (term_lens[i] < 1 || term_offsets[i] != total) {
+      delete ex;
+      return fail(SC_ERR_INVALID, "term %d: length %d / offset %d (expected offset %d)", i, term_lens[i], term_offsets[i], total);
+    }
+    total += term_lens[i];
+    degree = std::max(degree, static_cast<int>(term_lens[i]));
+  }
+  if (total > kMaxFlat) {
+    delete ex;
+    return fail(SC_ERR_UNSUPPORTED, "%d factors exceed %d", total, kMaxFlat);
+  }
+  if (degree > kMaxPoints - 1) {
+    delete ex;
+    return fail(SC_ERR_UNSUPPORTED, "degree %d exceeds %d", degree, kMaxPoints - 1);
+  }
+  for (int i = 0; i < total; ++i)
+    if (flat[i] < 0 || flat[i] >= num_vars) {
+      delete ex;
+      return fail(SC_ERR_INVALID, "factor %d refers to table %d of %d", i, flat[i], num_vars);
+    }
+  ex->degree = degree;
+  ex->coeffs.assign(num_terms, 0);
+  if (coeffs) ex->coeffs.assign(coeffs, coeffs + num_terms);
+  if (coeff_limbs) ex->coeff_limbs.assign(coeff_limbs, coeff_limbs + 8 * num_terms);
+  ex->lens.assign(term_lens, term_lens + num_terms);
+  ex->offs.assign(term_offsets, term_offsets + num_terms);
+  ex->flat.assign(flat, flat + total);
+  *out = ex;
+  return SC_OK;
+}
+
+int sc_expr_destroy(sc_expr* expr) {
+  delete expr;
+  return SC_OK;
+}
+
+int sc_expr_degree(const sc_expr* expr) { return expr ? expr->degree : -1; }
+int sc_expr_num_vars(const sc_expr* expr) { return expr ? expr->num_vars : -1; }
+
+int sc_tables_generate(sc_ctx* ctx, const sc_field* field, int num_tables, int num_rounds,
+                       const int32_t* kinds, uint64_t seed, uint32_t* tables_dev) {
+  if (!ctx || !field || !kinds || !tables_dev) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_tables < 1 || num_tables > kMaxVars) return fail(SC_ERR_INVALID, "num_tables %d outside 1..%d", num_tables, kMaxVars);
+  if (num_rounds < 1 || num_rounds > kMaxRounds) return fail(SC_ERR_INVALID, "num_rounds %d outside 1..%d", num_rounds, kMaxRounds);
+  for (int k = 0; k < num_tables; ++k)
+    if (kinds[k] < 0) return fail(SC_ERR_INVALID, "kinds[%d] = %d", k, kinds[k]);
+  if (reinterpret_cast<uintptr_t>(tables_dev) % 16) return fail(SC_ERR_INVALID, "tables_dev must be 16-byte aligned");
+  switch (field->hf.L) {
+    case 1: return generate_impl<1>(ctx, field, num_tables, num_rounds, kinds, seed, tables_dev);
+    case 2: return generate_impl<2>(ctx, field, num_tables, num_rounds, kinds, seed, tables_dev);
+    case 4: return generate_impl<4>(ctx, field, num_tables, num_rounds, kinds, seed, tables_dev);
+    default: return generate_impl<8>(ctx, field, num_tables, num_rounds, kinds, seed, tables_dev);
+  }
+}
+
+static int convert(sc_ctx* ctx, const sc_field* field, uint32_t* tables, uint64_t entries, int num_tables, bool to_mont) {
+  if (!ctx || !field || !tables) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_tables < 1 || entries == 0) return fail(SC_ERR_INVALID, "empty table set");
+  switch (field->hf.L) {
+    case 1: return convert_impl<1>(ctx, field, tables, entries, num_tables, to_mont);
+    case 2: return convert_impl<2>(ctx, field, tables, entries, num_tables, to_mont);
+    case 4: return convert_impl<4>(ctx, field, tables, entries, num_tables, to_mont);
+    default: return convert_impl<8>(ctx, field, tables, entries, num_tables, to_mont);
+  }
+}
+
+int sc_tables_to_mont(sc_ctx* ctx, const sc_field* field, uint32_t* tables_dev, uint64_t entries, int num_tables) {
+  return convert(ctx, field, tables_dev, entries, num_tables, true);
+}
+
+int sc_tables_from_mont(sc_ctx* ctx, const sc_field* field, uint32_t* tables_dev, uint64_t entries, int num_tables) {
+  return convert(ctx, field, tables_dev, entries, num_tables, false);
+}
+
+int sc_field_apply(sc_ctx* ctx, const sc_field* field, int op, const uint32_t* a_dev, const uint32_t* b_dev,
+                   uint32_t* out_dev, uint64_t count) {
+  if (!ctx || !field || !a_dev || !b_dev || !out_dev) return fail(SC_ERR_INVALID, "NULL argument");
+  if (op < 0 || op > 2) return fail(SC_ERR_INVALID, "unknown op %d", op);
+  if (count == 0) return SC_OK;
+  switch (field->hf.L) {
+    case 1: return apply_impl<1>(ctx, field, op, a_dev, b_dev, out_dev, count);
+    case 2: return apply_impl<2>(ctx, field, op, a_dev, b_dev, out_dev, count);
+    case 4: return apply_impl<4>(ctx, field, op, a_dev, b_dev, out_dev, count);
+    default: return apply_impl<8>(ctx, field, op, a_dev, b_dev, out_dev, count);
+  }
+}
+
+int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,
+             const uint32_t* tables_dev, int challenge_mode, const uint32_t* explicit_challenges,
+             uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
+             uint32_t* out_claim0, uint64_t* out_checksum) {
+  if (!ctx || !field || !expr || !tables_dev) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_rounds < 1 || num_rounds > kMaxRounds)
+    return fail(SC_ERR_INVALID, "num_rounds %d outside 1..%d", num_rounds, kMaxRounds);
+  if (challenge_mode < SC_CHALLENGE_SHA3 || challenge_mode > SC_CHALLENGE_EXPLICIT)
+    return fail(SC_ERR_INVALID, "unknown challenge mode %d", challenge_mode);
+  if (challenge_mode == SC_CHALLENGE_EXPLICIT && !explicit_challenges)
+    return fail(SC_ERR_INVALID, "explicit challenge mode needs explicit_challenges");
+  if (reinterpret_cast<uintptr_t>(tables_dev) % 16) return fail(SC_ERR_INVALID, "tables_dev must be 16-byte aligned");
+  if (field->device != ctx->device) return fail(SC_ERR_INVALID, "field was set up on device %d, context is on %d", field->device, ctx->device);
+  SC_CUDA(cudaSetDevice(ctx->device));
+  switch (field->hf.L) {
+    case 1: return prove_impl<1>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
+    case 2: return prove_impl<2>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
+    case 4: return prove_impl<4>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
+    default: return prove_impl<8>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
+  }
+}
+
+}  // extern "C"

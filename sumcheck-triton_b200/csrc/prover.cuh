@@ -1,0 +1,378 @@
+// The SumCheck round kernel and its finalisation.
+//
+// One launch per round j does the whole round, with no host round trip:
+//
+//   1. fold (j >= 1): each thread reads 4 consecutive entries of every table of round j-1
+//      (one 128-bit load per limb plane), folds them with r_{j-1} into the pair
+//      (T_j[2i], T_j[2i+1]) and writes that pair back (the fold of the previous round,
+//      reference field_sumcheck.cu:677-694, fused into this round's read);
+//   2. evaluate: extends every table's pair to t = 0..d (v(t) = v(t-1) + (o - e); reference
+//      field_sumcheck.cu:326-348) and evaluates the constraint at each point
+//      (field_sumcheck.cu:389-590), accumulating d+1 sums per thread;
+//   3. reduce: warp shuffles, then shared memory, then one partial per block in global
+//      memory; the last block to finish (atomic ticket) sums the partials -- a single-pass
+//      grid reduction in place of the reference's log-depth launch tree
+//      (field_sumcheck.cu:635-675, :996-1010);
+//   4. finalise (last block only): stores g_j(0..d), adds the round's checksum, derives r_j
+//      by SHA3 over the round polynomial on the device (field_sumcheck.cu:857-907) and, in
+//      the last round, the final claim g_{n-1}(r_{n-1}) and the folded values f_k(r).
+//
+// Tables are limb-planar: table k, limb l is the u32 plane at (k * L + l) * len.
+#pragma once
+#include <cstdint>
+
+#include "field.cuh"
+#include "keccak.cuh"
+
+namespace sc {
+
+constexpr int kMaxVars = 32;
+constexpr int kMaxTerms = 32;
+constexpr int kMaxFlat = 128;
+constexpr int kMaxRounds = 40;
+
+enum ChallengeMode : int32_t { kChallengeSha3 = 0, kChallengeFixed = 1, kChallengeExplicit = 2 };
+
+// Coefficient handling per term: +1 / -1 are an add / a subtract; other small values an
+// addition chain; anything else a product with the coefficient's Montgomery image.
+enum CoeffKind : uint8_t { kCoeffPlus = 0, kCoeffMinus = 1, kCoeffSmall = 2, kCoeffMont = 3 };
+
+// Constants of one field that only the finalisation needs (device memory, per field).
+struct FieldConsts {
+  uint32_t p[kMaxLimbs];
+  uint32_t np;
+  uint32_t limbs;
+  uint32_t p_small;                          // p if p < 2^32, else 0
+  uint32_t one[kMaxLimbs];                   // R mod p
+  uint32_t r2[kMaxLimbs];                    // R^2 mod p
+  uint32_t pts[kMaxPoints][kMaxLimbs];       // Montgomery image of t = 0..7
+  uint32_t kdig[8][kMaxLimbs];               // R^2 2^(32 i) mod p: digest word i
+  uint32_t lag[kMaxPoints][kMaxPoints][kMaxLimbs];  // lag[d][t] = 1 / prod_{s<=d, s!=t} (t - s)
+};
+
+// A compiled expression for one field (kernel parameter: lives in the constant bank).
+struct ExprDev {
+  int32_t num_vars;
+  int32_t num_terms;
+  int32_t degree;
+  int32_t pad;
+  uint8_t term_len[kMaxTerms];
+  uint8_t term_off[kMaxTerms];
+  uint8_t flat[kMaxFlat];
+  uint8_t coeff_kind[kMaxTerms];
+  int32_t coeff_small[kMaxTerms];
+  uint32_t coeff_mont[kMaxTerms][kMaxLimbs];
+};
+
+// Per-proof device state, all Montgomery limbs (written by the finalisation).
+struct ProofState {
+  uint32_t* counter;     // block tickets of the running round, reset to 0 after each round
+  uint64_t* checksum;    // sum over rounds and points of (i + 1) limb_i
+  uint32_t* polys;       // [n][kMaxPoints][L]
+  uint32_t* chals;       // [n][L]
+  uint32_t* finals;      // [1 + K][L]: g_{n-1}(r_{n-1}), then f_k(r) for every table
+  uint32_t* claim0;      // [L]
+  uint32_t* status;      // nonzero on a device-detected error
+};
+
+struct RoundArgs {
+  const uint32_t* src;   // T_{j-1} when folding, else T_j
+  uint32_t* dst;         // T_j when folding, else unused
+  uint64_t src_len;      // entries per plane of src
+  uint64_t pairs;        // N_j / 2
+  int32_t round;
+  int32_t num_rounds;
+  int32_t fold;
+  int32_t mode;          // ChallengeMode
+  uint32_t* partials;    // [gridDim.x][kMaxPoints][L]
+  const FieldConsts* fc;
+  ProofState st;
+};
+
+template <int L>
+__device__ __forceinline__ Fe<L> ld_fe(const uint32_t* p) {
+  Fe<L> r;
+#pragma unroll
+  for (int i = 0; i < L; ++i) r.w[i] = p[i];
+  return r;
+}
+
+template <int L>
+__device__ __forceinline__ Fe<L> ld_fe_cg(const uint32_t* p) {
+  Fe<L> r;
+#pragma unroll
+  for (int i = 0; i < L; ++i) r.w[i] = __ldcg(p + i);
+  return r;
+}
+
+template <int L>
+__device__ __forceinline__ void st_fe(uint32_t* p, const Fe<L>& a) {
+#pragma unroll
+  for (int i = 0; i < L; ++i) p[i] = a.w[i];
+}
+
+// Shared-memory element of thread `tid` in a [slot][limb][thread] array (conflict-free).
+template <int L>
+__device__ __forceinline__ Fe<L> sm_get(const uint32_t* sm, int slot, int tid, int nthr) {
+  Fe<L> r;
+#pragma unroll
+  for (int l = 0; l < L; ++l) r.w[l] = sm[(slot * L + l) * nthr + tid];
+  return r;
+}
+
+template <int L>
+__device__ __forceinline__ void sm_put(uint32_t* sm, int slot, int tid, int nthr, const Fe<L>& a) {
+#pragma unroll
+  for (int l = 0; l < L; ++l) sm[(slot * L + l) * nthr + tid] = a.w[l];
+}
+
+// Evaluate the runtime expression on the point values held in shared memory.
+template <int L>
+__device__ __forceinline__ Fe<L> eval_expr(const ExprDev& E, const uint32_t* sv, int tid, int nthr,
+                                           const FieldParams<L>& F) {
+  Fe<L> total = fe_zero<L>();
+  for (int i = 0; i < E.num_terms; ++i) {
+    const int off = E.term_off[i];
+    const int len = E.term_len[i];
+    Fe<L> prod = sm_get<L>(sv, E.flat[off], tid, nthr);
+    for (int f = 1; f < len; ++f) prod = fe_mul(prod, sm_get<L>(sv, E.flat[off + f], tid, nthr), F);
+    switch (E.coeff_kind[i]) {
+      case kCoeffPlus:
+        total = fe_add(total, prod, F);
+        break;
+      case kCoeffMinus:
+        total = fe_sub(total, prod, F);
+        break;
+      case kCoeffSmall: {
+        const int32_t c = E.coeff_small[i];
+        const Fe<L> s = fe_mul_small(prod, c < 0 ? -c : c, F);
+        total = c < 0 ? fe_sub(total, s, F) : fe_add(total, s, F);
+        break;
+      }
+      default: {
+        Fe<L> cm;
+#pragma unroll
+        for (int l = 0; l < L; ++l) cm.w[l] = E.coeff_mont[i][l];
+        total = fe_add(total, fe_mul(prod, cm, F), F);
+      }
+    }
+  }
+  return total;
+}
+
+// Reduce acc[0..d] over the block; the block sums land in red_out[t * L + l] (shared).
+template <int L>
+__device__ __forceinline__ void block_reduce(Fe<L> (&acc)[kMaxPoints], int d, uint32_t* scratch,
+                                             uint32_t* red_out, const FieldParams<L>& F) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+#pragma unroll
+  for (int t = 0; t < kMaxPoints; ++t) {
+    if (t > d) break;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[t] = fe_add(acc[t], fe_shfl_down(acc[t], off), F);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) {
+      if (t > d) break;
+      st_fe<L>(scratch + (warp * kMaxPoints + t) * L, acc[t]);
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) {
+      if (t > d) break;
+      Fe<L> v = lane < nwarps ? ld_fe<L>(scratch + (lane * kMaxPoints + t) * L) : fe_zero<L>();
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v = fe_add(v, fe_shfl_down(v, off), F);
+      if (lane == 0) st_fe<L>(red_out + t * L, v);
+    }
+  }
+  __syncthreads();
+}
+
+template <int L>
+__device__ __forceinline__ Fe<L> fc_get(const uint32_t* row) {
+  return ld_fe<L>(row);
+}
+
+// Last block of a round: g_j is in g_sm[t * L + l]. Warp 0 does all of this.
+template <int L>
+__device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const FieldParams<L>& F,
+                               const uint32_t* g_sm, uint8_t* msg) {
+  const int lane = threadIdx.x & 31;
+  const int d = E.degree;
+  const int j = A.round;
+  const FieldConsts& fc = *A.fc;
+  // 1. round polynomial and checksum
+  for (int i = lane; i < (d + 1) * L; i += 32) A.st.polys[(j * kMaxPoints + i / L) * L + i % L] = g_sm[i];
+  if (lane == 0) {
+    uint64_t cs = 0;
+    for (int t = 0; t <= d; ++t)
+      for (int l = 0; l < L; ++l) cs += static_cast<uint64_t>(l + 1) * g_sm[t * L + l];
+    *A.st.checksum += cs;
+    if (j == 0) {
+      const Fe<L> c0 = fe_add(ld_fe<L>(g_sm), ld_fe<L>(g_sm + L), F);
+      st_fe<L>(A.st.claim0, c0);
+    }
+  }
+  // 2. challenge r_j
+  Fe<L> r;
+  if (A.mode == kChallengeSha3) {
+    const char dom[] = "zkduel:field-sweep:v1";
+    constexpr int kDom = sizeof(dom) - 1;
+    const int nwords = 1 + (d + 1) * L;
+    if (lane < kDom) msg[lane] = static_cast<uint8_t>(dom[lane]);
+    for (int i = lane; i < nwords; i += 32) {
+      const uint32_t w = i == 0 ? static_cast<uint32_t>(j) : g_sm[i - 1];
+      msg[kDom + 4 * i + 0] = static_cast<uint8_t>(w);
+      msg[kDom + 4 * i + 1] = static_cast<uint8_t>(w >> 8);
+      msg[kDom + 4 * i + 2] = static_cast<uint8_t>(w >> 16);
+      msg[kDom + 4 * i + 3] = static_cast<uint8_t>(w >> 24);
+    }
+    __syncwarp();
+    uint32_t dig[8];
+    sha3_256_warp(msg, kDom + 4 * nwords, dig);
+    // digest (little-endian 256-bit D) -> D R mod p = sum_i (w_i mod p) * R^2 2^(32 i) / R
+    Fe<L> term = fe_zero<L>();
+    if (lane < 8) {
+      uint32_t w = dig[0];
+#pragma unroll
+      for (int i = 1; i < 8; ++i)
+        if (lane == i) w = dig[i];
+      if (fc.p_small) w %= fc.p_small;
+      Fe<L> wf = fe_zero<L>();
+      wf.w[0] = w;
+      term = fe_mul(wf, fc_get<L>(fc.kdig[lane]), F);
+    }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) term = fe_add(term, fe_shfl_down(term, off), F);
+    r = fe_shfl(term, 0);
+    if (lane == 0) st_fe<L>(A.st.chals + j * L, r);
+  } else if (A.mode == kChallengeFixed) {
+    r = fc_get<L>(fc.one);
+    if (lane == 0) st_fe<L>(A.st.chals + j * L, r);
+  } else {
+    r = ld_fe<L>(A.st.chals + j * L);
+  }
+  // 3. last round: final claim g(r) by Lagrange interpolation, and f_k(r) per table
+  if (j == A.num_rounds - 1) {
+    Fe<L> term = fe_zero<L>();
+    if (lane <= d) {
+      term = fe_mul(ld_fe<L>(g_sm + lane * L), fc_get<L>(fc.lag[d][lane]), F);
+      for (int s = 0; s <= d; ++s)
+        if (s != lane) term = fe_mul(term, fe_sub(r, fc_get<L>(fc.pts[s]), F), F);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) term = fe_add(term, fe_shfl_down(term, off), F);
+    if (lane == 0) st_fe<L>(A.st.finals, term);
+    const uint32_t* tab = A.fold ? A.dst : A.src;  // T_{n-1}: 2 entries per plane
+    for (int k = lane; k < E.num_vars; k += 32) {
+      Fe<L> e, o;
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        e.w[l] = __ldcg(tab + (k * L + l) * 2 + 0);
+        o.w[l] = __ldcg(tab + (k * L + l) * 2 + 1);
+      }
+      const Fe<L> f = fe_add(e, fe_mul(r, fe_sub(o, e, F), F), F);
+      st_fe<L>(A.st.finals + (1 + k) * L, f);
+    }
+  }
+}
+
+// Dynamic shared memory per thread: values and differences of every table.
+__host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { return 2 * K * L; }
+
+template <int L>
+__global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const ExprDev E,
+                                                    const FieldParams<L> F) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
+  __shared__ __align__(16) uint8_t msg[3 * 136];
+  __shared__ int is_last;
+
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int K = E.num_vars;
+  const int d = E.degree;
+  uint32_t* sv = smem;              // [K][L][nthr] values at the current point
+  uint32_t* sd = smem + K * L * nthr;  // [K][L][nthr] differences o - e
+
+  Fe<L> acc[kMaxPoints];
+#pragma unroll
+  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+
+  Fe<L> r_prev = fe_zero<L>();
+  if (A.fold) r_prev = ld_fe_cg<L>(A.st.chals + (A.round - 1) * L);
+
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * nthr;
+  for (uint64_t q = static_cast<uint64_t>(blockIdx.x) * nthr + tid; q < A.pairs; q += stride) {
+    // load (and fold) the pair of every table
+    for (int k = 0; k < K; ++k) {
+      Fe<L> e, o;
+      if (A.fold) {
+        Fe<L> x0, x1, x2, x3;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          const uint4 v = __ldcs(reinterpret_cast<const uint4*>(A.src + (static_cast<uint64_t>(k) * L + l) * A.src_len) + q);
+          x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
+        }
+        e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
+        o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
+        const uint64_t dst_len = A.src_len >> 1;
+#pragma unroll
+        for (int l = 0; l < L; ++l)
+          reinterpret_cast<uint2*>(A.dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+      } else {
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          const uint2 v = __ldcs(reinterpret_cast<const uint2*>(A.src + (static_cast<uint64_t>(k) * L + l) * A.src_len) + q);
+          e.w[l] = v.x; o.w[l] = v.y;
+        }
+      }
+      sm_put<L>(sv, k, tid, nthr, e);
+      sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
+    }
+    // extend to t = 0..d and evaluate
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) {
+      if (t > d) break;
+      if (t > 0) {
+        for (int k = 0; k < K; ++k)
+          sm_put<L>(sv, k, tid, nthr, fe_add(sm_get<L>(sv, k, tid, nthr), sm_get<L>(sd, k, tid, nthr), F));
+      }
+      acc[t] = fe_add(acc[t], eval_expr<L>(E, sv, tid, nthr, F), F);
+    }
+  }
+
+  // block partial -> global; the last block reduces all partials
+  __syncthreads();
+  block_reduce<L>(acc, d, smem, g_sm, F);
+  if (tid < (d + 1) * L) A.partials[static_cast<uint64_t>(blockIdx.x) * kMaxPoints * L + tid] = g_sm[tid];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) is_last = (atomicAdd(A.st.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+
+#pragma unroll
+  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+  for (uint32_t b = tid; b < gridDim.x; b += nthr) {
+    const uint32_t* pb = A.partials + static_cast<uint64_t>(b) * kMaxPoints * L;
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) {
+      if (t > d) break;
+      acc[t] = fe_add(acc[t], ld_fe_cg<L>(pb + t * L), F);
+    }
+  }
+  block_reduce<L>(acc, d, smem, g_sm, F);
+  if (tid < 32) finalize_round<L>(A, E, F, g_sm, msg);
+  if (tid == 0) {
+    __threadfence();
+    *A.st.counter = 0;
+  }
+}
+
+}  // namespace sc
