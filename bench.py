@@ -1,0 +1,446 @@
+"""Benchmark: SumCheck proofs/s on the mixed 512-proof stream, one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--path batched|plain]
+
+A step proves the whole stream once: 512 independent proofs, num_vars uniform in {10..20},
+64- or 256-bit field by coin flip, random sum-of-products expressions of degree 2-6 over
+2-8 uniform tables (zkduel_b200.streams.batched_stream, master seed 0; rank r uses master
+seed r, so per-GPU work is fixed: weak scaling, no collective on the data path).
+
+Prints one JSON line (rank 0):
+  value      proofs/s over all ranks, tables resident in HBM before the timed region,
+             timed with CUDA events on the proving stream, max over ranks;
+  e2e        the same through the host-buffer API: every step copies each proof's tables
+             from pinned host memory and reads each proof's results back;
+  plain      the same stream proved one proof at a time (the denominator of the batched
+             speed-up);
+  roofline   the dominant round kernel (by time) against its bound: integer multiply-adds
+             against the measured IMAD rate (256-bit) or bytes against measured HBM GB/s;
+  cpu_baseline  the C oracle (all host threads) on a bounded sample of the same stream.
+--impl reference times that CPU port alone on the same workload (the reference's own
+prover is Python-only and cannot run here; the port restates it and is pinned against it).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "sumcheck-triton_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "sumcheck_proofs_per_s_mixed_stream"
+WORKLOAD = "batched_512"
+STREAM_COUNT = 512
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--path", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default=None,
+                    help="profile mode: prove one plain config (plain_p32|plain_goldilocks|plain_bls) twice and exit")
+    ap.add_argument("--case-vars", type=int, default=None, help="num_vars for --case (default: the config's)")
+    return ap.parse_args()
+
+
+def profile_case(args) -> int:
+    """One plain proof, twice (first warms up); for ncu captures of the round kernel."""
+    import torch
+
+    from zkduel_b200 import api
+    from zkduel_b200.configs import PLAIN_CONFIGS
+    from zkduel_b200.fields import get_field
+
+    cfg = PLAIN_CONFIGS[args.case]
+    n = args.case_vars or cfg.num_vars
+    spec = get_field(cfg.bit_width)
+    enc = api.encode_expression(cfg.expression)
+    kinds = [api._lib.SC_TABLE_BERNOULLI if k == "bernoulli" else api._lib.SC_TABLE_UNIFORM for k in cfg.table_kinds()]
+    t = api.generate_tables(spec, enc.num_vars, n, kinds, cfg.seed)
+    expr = api.CompiledExpression(enc, spec.modulus)
+    times = []
+    for _ in range(2):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        p = api.prove_device(t, expr, spec, n, "sha3")
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    print(json.dumps({"case": args.case, "num_vars": n, "ms": times, "checksum": p.checksum}))
+    return 0
+
+
+# ------------------------------------------------------------------------------ helpers
+
+
+def measured_peaks() -> dict:
+    try:
+        return json.loads(PEAKS.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if _cuda_ok() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def _cuda_ok() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------ workload
+
+
+class Workload:
+    """The stream's proofs with their tables resident on the device."""
+
+    def __init__(self, master_seed: int, device):
+        import torch
+
+        from zkduel_b200 import api
+        from zkduel_b200.fields import get_field
+        from zkduel_b200.streams import batched_stream
+
+        self.specs = batched_stream(STREAM_COUNT, master_seed)
+        self.items = []
+        for s in self.specs:
+            spec = get_field(s.bit_width)
+            enc = s.encoded()
+            expr = api.CompiledExpression(enc, spec.modulus)
+            tables = api.generate_tables(spec, enc.num_vars, s.num_vars, [api._lib.SC_TABLE_UNIFORM] * enc.num_vars,
+                                         s.seed, device)
+            self.items.append((s, spec, expr, tables))
+        torch.cuda.synchronize(device)
+
+    def table_bytes(self) -> int:
+        return sum(t.numel() * 4 for _s, _f, _e, t in self.items)
+
+
+def run_plain(work: Workload):
+    from zkduel_b200 import api
+
+    out = []
+    for s, spec, expr, tables in work.items:
+        out.append(api.prove_device(tables, expr, spec, s.num_vars, "sha3"))
+    return out
+
+
+def run_batched(work: Workload, batcher):
+    return batcher.run()
+
+
+def timed(fn, steps: int, world: int, device):
+    import torch
+
+    barrier(world)
+    torch.cuda.synchronize(device)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        fn()
+    end.record()
+    torch.cuda.synchronize(device)
+    barrier(world)
+    return start.elapsed_time(end)
+
+
+# ------------------------------------------------------------------------------ CPU port
+
+
+def cpu_port_sample(budget_s: float, master_seed: int = 0, sample_stride: int = 16, max_proofs: int | None = None):
+    """The C oracle with every host thread on proofs 0, stride, 2 stride, ... of the stream
+    until ``budget_s`` of proving time is spent. Returns (proofs/s, proofs, seconds, threads)."""
+    from oracle import c_oracle as C
+    from oracle import oracle as O
+    from zkduel_b200.fields import get_field
+    from zkduel_b200.streams import batched_stream
+
+    threads = os.cpu_count() or 1
+    specs = batched_stream(STREAM_COUNT, master_seed)[::sample_stride]
+    done, spent = 0, 0.0
+    for s in specs:
+        f = get_field(s.bit_width)
+        terms, k = O.indexed_terms(s.expression)
+        t = C.generate(f.modulus, f.limbs, [0] * k, s.num_vars, s.seed)
+        t0 = time.perf_counter()
+        C.prove(terms, k, f.modulus, f.limbs, t, "sha3", threads=threads)
+        spent += time.perf_counter() - t0
+        done += 1
+        if spent >= budget_s or (max_proofs and done >= max_proofs):
+            break
+    return done / spent, done, spent, threads
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    per_step = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        rate, done, spent, threads = cpu_port_sample(budget_s=8.0, max_proofs=12)
+        info = (done, threads)
+        if i >= args.warmup:
+            per_step.append(done / rate)
+    total = sum(per_step)
+    done, threads = info
+    value = done * len(per_step) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(per_step),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Montgomery)",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "proofs_per_step": done,
+                                        "sample": f"proofs 0, 16, 32, ... of the 512-proof stream (first {done})"},
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
+                         "sample": f"{done} proofs (every 16th of the stream) per step"},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ main
+
+
+def main() -> int:
+    args = parse()
+    if args.case:
+        return profile_case(args)
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+
+    from zkduel_b200 import api, roofline
+    from zkduel_b200.fields import get_field
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    work = Workload(master_seed=rank, device=device)
+    ctx = api.get_context(device)
+    imad_rate = api.calibrate_imad(ctx)
+
+    batcher = None
+    path = args.path
+    if path == "batched":
+        try:
+            from zkduel_b200 import batch
+
+            batcher = batch.BatchProver([(s.expression, s.bit_width, s.num_vars, t) for s, _f, _e, t in work.items],
+                                        device=device)
+        except (ImportError, AttributeError):
+            path = "plain"
+    step = (lambda: run_batched(work, batcher)) if path == "batched" else (lambda: run_plain(work))
+
+    for _ in range(args.warmup):
+        step()
+    ctx.set_timing(True)
+    with ClockSampler(local) as clocks:
+        ms = timed(step, args.steps, world, device)
+    launch_ms = ctx.launch_times()
+    ctx.set_timing(False)
+    ms_step = max_over_ranks(ms / args.steps, world)
+    value = world * STREAM_COUNT / (ms_step / 1e3)
+
+    # roofline of the dominant kernel class, from the launches of the timed region
+    per_class = {}
+    launches = []
+    for s, spec, _e, _t in work.items:
+        enc = s.encoded()
+        M = roofline.products_per_point(s.expression)
+        for j in range(s.num_vars):
+            launches.append((spec.limbs, roofline.launch_bytes(enc.num_vars, spec.limbs, s.num_vars, j),
+                             roofline.launch_imad(enc.num_vars, spec.limbs, enc.degree, M, s.num_vars, j)))
+    if path == "plain" and len(launch_ms) == len(launches) * args.steps:
+        for i, t in enumerate(launch_ms):
+            L, b, im = launches[i % len(launches)]
+            c = per_class.setdefault(L, {"ms": 0.0, "bytes": 0, "imad": 0, "launches": 0})
+            c["ms"] += t
+            c["bytes"] += b
+            c["imad"] += im
+            c["launches"] += 1
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    roof = None
+    if per_class:
+        L, c = max(per_class.items(), key=lambda kv: kv[1]["ms"])
+        if L >= 4:
+            ach = c["imad"] / (c["ms"] / 1e3) / 1e12
+            pk = imad_rate / 1e12
+            roof = {"bound": "imad", "kernel": f"round_kernel<{L}>", "achieved": ach, "peak": pk,
+                    "unit": "TIMAD/s", "frac": ach / pk, "traffic": None,
+                    "peak_source": "sc_calibrate_imad probe (measured live)"}
+        else:
+            ach = c["bytes"] / (c["ms"] / 1e3) / 1e9
+            roof = {"bound": "hbm", "kernel": f"round_kernel<{L}>", "achieved": ach, "peak": hbm_peak,
+                    "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+        roof["by_class"] = {f"L{k}": {"ms": v["ms"], "launches": v["launches"],
+                                      "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
+                                      "TIMAD/s": v["imad"] / (v["ms"] / 1e3) / 1e12} for k, v in per_class.items()}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (Montgomery; 64- and 256-bit fields)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "path": path, "proofs_per_step_per_gpu": STREAM_COUNT,
+                   "table_bytes_per_gpu": work.table_bytes(),
+                   "l2": "inputs larger than L2 (tables total > 126 MB); no flush", "parallelism": f"replicas x{world}"},
+        "gpu_launches": len(launch_ms) if path == "plain" else None,
+        "clocks": clocks.summary(),
+        "imad_peak_tera_per_s": imad_rate / 1e12,
+    }
+    if roof:
+        line["roofline"] = roof
+
+    if rank == 0 and world == 1 and not args.no_e2e:
+        line["e2e"] = e2e_measure(work, args, device)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, done, spent, threads = cpu_port_sample(budget_s=15.0)
+        line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
+                                "sample": f"{done} proofs (every 16th of the 512-proof stream), {spent:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_measure(work: Workload, args, device) -> dict:
+    """Host-buffer path: per step, copy every proof's canonical tables from pinned host
+    memory, convert on the device, prove, read the results back."""
+    import torch
+
+    from zkduel_b200 import api
+
+    host = []
+    for s, spec, _e, t in work.items:
+        canon = api.download_tables(t, spec)
+        h = torch.from_numpy(canon.view("int32")).pin_memory()
+        host.append(h)
+    h2d = sum(h.numel() * 4 for h in host)
+
+    def step():
+        res = []
+        for (s, spec, expr, _t), h in zip(work.items, host):
+            res.append(api.prove_host(h, expr, spec, s.num_vars, "sha3", device=device))
+        return res
+
+    step()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    steps = max(1, min(args.steps, 3))
+    d2h = 0
+    for _ in range(steps):
+        res = step()
+    torch.cuda.synchronize(device)
+    dt = (time.perf_counter() - t0) / steps
+    for p in res:
+        d2h += p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
+    return {"value": STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": dt * 1e3, "path": "plain (host buffers)", "steps": steps}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

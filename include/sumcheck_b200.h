@@ -71,6 +71,13 @@ int sc_ctx_create(int device, void* stream, sc_ctx** out);
 int sc_ctx_destroy(sc_ctx* ctx);
 /* Waits for all work of the context's stream. */
 int sc_ctx_synchronize(sc_ctx* ctx);
+/* Per-launch device timing of the round kernels (CUDA events on the context's stream),
+ * off by default. sc_ctx_launch_times sets *count to the number of recorded launch
+ * durations (ms, issue order, for launches completed by the last synchronising call) and
+ * moves the first min(count, capacity) of them into out_ms (NULL: only counts). The reference's equivalent is its
+ * --timing-mode round-sum / --timer events (field_sumcheck.cu:1032-1080, :1237-1246). */
+int sc_ctx_set_timing(sc_ctx* ctx, int enable);
+int sc_ctx_launch_times(sc_ctx* ctx, float* out_ms, int capacity, int* count);
 
 /* A field of modulus p (L limbs) with nprime = -p^-1 mod 2^32. Rejects, with
  * SC_ERR_UNSAFE_MODULUS, the moduli the reference's guard rejects: even or < 3, wrong
@@ -115,6 +122,12 @@ int sc_tables_from_mont(sc_ctx* ctx, const sc_field* field, uint32_t* tables_dev
  * (src/zkduel/triton_backend/uint256.py:1149-1313). Asynchronous. */
 int sc_field_apply(sc_ctx* ctx, const sc_field* field, int op, const uint32_t* a_dev,
                    const uint32_t* b_dev, uint32_t* out_dev, uint64_t count);
+
+/* Measures the device's 32-bit integer multiply-add rate (IMAD/s) with a probe kernel of
+ * independent mad.lo / mad.hi chains (the instruction pair of the Montgomery product);
+ * the denominator of the integer-pipe roofline. Synchronous, about a millisecond.
+ * No counterpart in the reference (it reports no roofline). */
+int sc_calibrate_imad(sc_ctx* ctx, double* out_imad_per_s);
 
 /* One SumCheck proof over num_rounds variables: num_rounds launches, no host round trip,
  * then one copy of the results to the host (the call returns when they are there).

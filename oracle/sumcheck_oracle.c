@@ -331,23 +331,19 @@ static void* run_job(void* arg) {
 
 static void run_parallel(job_t* jobs, int threads, uint64_t count) {
   pthread_t th[256];
-  int used = 0;
+  int created[256] = {0};
   uint64_t per = (count + threads - 1) / threads;
   for (int t = 0; t < threads; ++t) {
     jobs[t].lo = per * t < count ? per * t : count;
     jobs[t].hi = per * (t + 1) < count ? per * (t + 1) : count;
   }
   for (int t = 1; t < threads; ++t)
-    if (jobs[t].lo < jobs[t].hi && pthread_create(&th[t], NULL, run_job, &jobs[t]) == 0) used |= 0, jobs[t].phase |= 0x100;
+    if (jobs[t].lo < jobs[t].hi) created[t] = pthread_create(&th[t], NULL, run_job, &jobs[t]) == 0;
   run_job(&jobs[0]);
-  for (int t = 1; t < threads; ++t)
-    if (jobs[t].phase & 0x100) {
-      pthread_join(th[t], NULL);
-      jobs[t].phase &= 0xFF;
-    } else if (jobs[t].lo < jobs[t].hi) {
-      run_job(&jobs[t]);
-    }
-  (void)used;
+  for (int t = 1; t < threads; ++t) {
+    if (created[t]) pthread_join(th[t], NULL);
+    else if (jobs[t].lo < jobs[t].hi) run_job(&jobs[t]);
+  }
 }
 
 /*
@@ -406,6 +402,7 @@ int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, 
       J->nxt = nxt;
       J->N = N;
       J->phase = 0;
+      memset(J->acc, 0, sizeof(J->acc)); /* a job with an empty range contributes zero */
     }
     run_parallel(jobs, half < (uint64_t)threads ? 1 : threads, half);
     uint32_t g[MAXP][MAXL];

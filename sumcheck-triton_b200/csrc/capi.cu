@@ -59,6 +59,11 @@ struct sc_ctx {
   DevBuf fold_a, fold_b, partials, state;
   uint32_t* host_state = nullptr;  // pinned staging of the proof state
   size_t host_state_bytes = 0;
+  // per-launch timing of the round kernels (off by default)
+  bool timing = false;
+  std::vector<cudaEvent_t> events;   // 2 per launch
+  int events_used = 0;
+  std::vector<float> launch_ms;      // durations of the launches since the last read
 };
 
 struct sc_field {
@@ -93,6 +98,37 @@ int ensure(sc_ctx* ctx, DevBuf& b, size_t bytes) {
     return fail(SC_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
   }
   b.bytes = want;
+  return SC_OK;
+}
+
+// Events bracketing one launch when timing is on (pool grows as needed).
+int timing_begin(sc_ctx* ctx, cudaEvent_t* start) {
+  if (!ctx->timing) return SC_OK;
+  while (static_cast<int>(ctx->events.size()) < ctx->events_used + 2) {
+    cudaEvent_t e;
+    SC_CUDA(cudaEventCreate(&e));
+    ctx->events.push_back(e);
+  }
+  *start = ctx->events[ctx->events_used++];
+  SC_CUDA(cudaEventRecord(*start, ctx->stream));
+  return SC_OK;
+}
+
+int timing_end(sc_ctx* ctx) {
+  if (!ctx->timing) return SC_OK;
+  SC_CUDA(cudaEventRecord(ctx->events[ctx->events_used++], ctx->stream));
+  return SC_OK;
+}
+
+// After a synchronisation: turn recorded event pairs into durations.
+int timing_collect(sc_ctx* ctx) {
+  if (!ctx->timing) return SC_OK;
+  for (int i = 0; i + 1 < ctx->events_used; i += 2) {
+    float ms = 0.f;
+    SC_CUDA(cudaEventElapsedTime(&ms, ctx->events[i], ctx->events[i + 1]));
+    ctx->launch_ms.push_back(ms);
+  }
+  ctx->events_used = 0;
   return SC_OK;
 }
 
@@ -275,8 +311,11 @@ int prove_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const u
     }
     const uint64_t want = (A.pairs + threads - 1) / threads;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
+    cudaEvent_t ev;
+    if ((rc = timing_begin(ctx, &ev))) return rc;
     round_kernel<L><<<grid, threads, smem, ctx->stream>>>(A, E, F);
     SC_CUDA(cudaGetLastError());
+    if ((rc = timing_end(ctx))) return rc;
   }
   // results
   if (ctx->host_state_bytes < so.total_words * 4) {
@@ -288,6 +327,7 @@ int prove_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const u
   }
   SC_CUDA(cudaMemcpyAsync(ctx->host_state, st, so.total_words * 4, cudaMemcpyDeviceToHost, ctx->stream));
   SC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if ((rc = timing_collect(ctx))) return rc;
   const uint32_t* hs = ctx->host_state;
   if (hs[so.status]) return fail(SC_ERR_DEVICE, "device status %u", hs[so.status]);
   if (out_polys)
@@ -398,6 +438,7 @@ int sc_ctx_destroy(sc_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->fold_a, &ctx->fold_b, &ctx->partials, &ctx->state})
     if (b->p) cudaFree(b->p);
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->host_state) cudaFreeHost(ctx->host_state);
   delete ctx;
   return SC_OK;
@@ -406,6 +447,25 @@ int sc_ctx_destroy(sc_ctx* ctx) {
 int sc_ctx_synchronize(sc_ctx* ctx) {
   if (!ctx) return fail(SC_ERR_INVALID, "ctx is NULL");
   SC_CUDA(cudaStreamSynchronize(ctx->stream));
+  return timing_collect(ctx);
+}
+
+int sc_ctx_set_timing(sc_ctx* ctx, int enable) {
+  if (!ctx) return fail(SC_ERR_INVALID, "ctx is NULL");
+  SC_CUDA(cudaStreamSynchronize(ctx->stream));
+  int rc = timing_collect(ctx);
+  ctx->timing = enable != 0;
+  ctx->launch_ms.clear();
+  return rc;
+}
+
+int sc_ctx_launch_times(sc_ctx* ctx, float* out_ms, int capacity, int* count) {
+  if (!ctx || !count) return fail(SC_ERR_INVALID, "NULL argument");
+  const int n = static_cast<int>(ctx->launch_ms.size());
+  *count = n;
+  const int take = out_ms ? std::min(n, std::max(capacity, 0)) : 0;
+  for (int i = 0; i < take; ++i) out_ms[i] = ctx->launch_ms[i];
+  ctx->launch_ms.erase(ctx->launch_ms.begin(), ctx->launch_ms.begin() + take);
   return SC_OK;
 }
 
@@ -598,6 +658,35 @@ int sc_field_apply(sc_ctx* ctx, const sc_field* field, int op, const uint32_t* a
     case 4: return apply_impl<4>(ctx, field, op, a_dev, b_dev, out_dev, count);
     default: return apply_impl<8>(ctx, field, op, a_dev, b_dev, out_dev, count);
   }
+}
+
+int sc_calibrate_imad(sc_ctx* ctx, double* out_imad_per_s) {
+  if (!ctx || !out_imad_per_s) return fail(SC_ERR_INVALID, "NULL argument");
+  SC_CUDA(cudaSetDevice(ctx->device));
+  uint32_t* sink = nullptr;
+  SC_CUDA(cudaMalloc(&sink, 16));
+  const int threads = 512, iters = 4096;
+  const int blocks = ctx->sm_count * 4;
+  cudaEvent_t e0, e1;
+  SC_CUDA(cudaEventCreate(&e0));
+  SC_CUDA(cudaEventCreate(&e1));
+  imad_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(sink, 64, 1u);  // warm-up
+  float best = 0.f;
+  for (int rep = 0; rep < 3; ++rep) {
+    SC_CUDA(cudaEventRecord(e0, ctx->stream));
+    imad_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(sink, iters, 7u + rep);
+    SC_CUDA(cudaEventRecord(e1, ctx->stream));
+    SC_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (best == 0.f || ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  const double ops = static_cast<double>(blocks) * threads * iters * 8.0 * 2.0;
+  *out_imad_per_s = ops / (best * 1e-3);
+  return SC_OK;
 }
 
 int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,

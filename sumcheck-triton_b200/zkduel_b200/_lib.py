@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_char_p, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
 from .fields import UnsafeModulusError
@@ -42,6 +42,8 @@ SIGNATURES = {
     "sc_ctx_create": (c_int, [c_int, c_void_p, POINTER(c_void_p)]),
     "sc_ctx_destroy": (c_int, [c_void_p]),
     "sc_ctx_synchronize": (c_int, [c_void_p]),
+    "sc_ctx_set_timing": (c_int, [c_void_p, c_int]),
+    "sc_ctx_launch_times": (c_int, [c_void_p, POINTER(c_float), c_int, POINTER(c_int)]),
     "sc_field_init": (c_int, [c_int, U32P, c_uint32, POINTER(c_void_p)]),
     "sc_field_destroy": (c_int, [c_void_p]),
     "sc_expr_compile": (
@@ -55,6 +57,7 @@ SIGNATURES = {
     "sc_tables_to_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_tables_from_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_field_apply": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_uint64]),
+    "sc_calibrate_imad": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_prove": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, U32P, U32P, U32P, U32P, U32P, U64P],

@@ -18,7 +18,7 @@ from typing import Iterable, Mapping, Sequence
 import numpy as np
 
 from . import _lib
-from .expression import EncodedExpression, Expression, encode_expression, expression_vars
+from .expression import EncodedExpression, Expression, encode_expression, expression_vars  # noqa: F401
 from .fields import FieldSpec, field_for_modulus, from_limbs, get_field
 
 BACKEND = "b200"
@@ -64,6 +64,18 @@ class Context:
 
     def synchronize(self) -> None:
         _lib.check(_lib.load().sc_ctx_synchronize(self.handle), "sc_ctx_synchronize")
+
+    def set_timing(self, enable: bool) -> None:
+        _lib.check(_lib.load().sc_ctx_set_timing(self.handle, int(bool(enable))), "sc_ctx_set_timing")
+
+    def launch_times(self) -> list[float]:
+        """Durations (ms) of the round-kernel launches since timing was enabled or last read."""
+        lib = _lib.load()
+        count = ctypes.c_int(0)
+        _lib.check(lib.sc_ctx_launch_times(self.handle, None, 0, ctypes.byref(count)), "sc_ctx_launch_times")
+        buf = (ctypes.c_float * max(1, count.value))()
+        _lib.check(lib.sc_ctx_launch_times(self.handle, buf, count.value, ctypes.byref(count)), "sc_ctx_launch_times")
+        return list(buf)[: count.value]
 
     def close(self) -> None:
         if self.handle:
@@ -327,6 +339,31 @@ def prove_device(tables, expr: CompiledExpression | Expression, spec: FieldSpec,
                               explicit, p(polys), p(chals), p(finals), p(claim0), ctypes.byref(checksum))
     _lib.check(rc, "sc_prove")
     return Proof(spec, n, d, tuple(var_names or enc.var_names), polys, chals, finals, claim0, int(checksum.value))
+
+
+def prove_host(host_tables, expr: CompiledExpression | Expression, spec: FieldSpec, num_rounds: int,
+               challenge_mode: str = "sha3", challenges: Sequence[int] | None = None, device=None) -> Proof:
+    """Prove from canonical host tables: an int32 (K, L, 2^n) tensor of limbs (pinned memory
+    for an asynchronous copy) or a uint32 numpy array. Copies them to the device, converts
+    them to Montgomery form there and proves; the results come back to the host."""
+    torch = _torch()
+    if isinstance(host_tables, np.ndarray):
+        host_tables = torch.from_numpy(np.ascontiguousarray(host_tables).view(np.int32))
+    ctx = get_context(device)
+    fld = get_device_field(spec, ctx.device)
+    dev = host_tables.to(torch.device("cuda", ctx.device), non_blocking=True)
+    K, _L, N = dev.shape
+    rc = _lib.load().sc_tables_to_mont(ctx.handle, fld.handle, ctypes.c_void_p(dev.data_ptr()), ctypes.c_uint64(N), int(K))
+    _lib.check(rc, "sc_tables_to_mont")
+    return prove_device(dev, expr, spec, num_rounds, challenge_mode, challenges)
+
+
+def calibrate_imad(ctx: Context | None = None) -> float:
+    """Measured 32-bit multiply-add rate of the device (IMAD/s), the integer-pipe peak."""
+    ctx = ctx or get_context()
+    out = ctypes.c_double(0.0)
+    _lib.check(_lib.load().sc_calibrate_imad(ctx.handle, ctypes.byref(out)), "sc_calibrate_imad")
+    return float(out.value)
 
 
 def sumcheck(
