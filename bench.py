@@ -223,10 +223,6 @@ def run_plain(work: Workload):
     return out
 
 
-def run_batched(work: Workload, batcher):
-    return batcher.run()
-
-
 def timed(fn, steps: int, world: int, device):
     import torch
 
@@ -319,45 +315,65 @@ def main() -> int:
     ctx = api.get_context(device)
     imad_rate = api.calibrate_imad(ctx)
 
-    batcher = None
+    from zkduel_b200.batch import BatchProver
+
+    batcher = BatchProver([(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items], device=device)
+    steps_fn = {"batched": batcher.run, "plain": lambda: run_plain(work)}
+
+    def measure(path, steps):
+        for _ in range(args.warmup):
+            steps_fn[path]()
+        if path == "plain":
+            ctx.set_timing(True)
+        with ClockSampler(local) as clk:
+            ms = timed(steps_fn[path], steps, world, device)
+        launch_ms = ctx.launch_times() if path == "plain" else None
+        if path == "plain":
+            ctx.set_timing(False)
+        return max_over_ranks(ms / steps, world), launch_ms, clk
+
     path = args.path
-    if path == "batched":
-        try:
-            from zkduel_b200 import batch
-
-            batcher = batch.BatchProver([(s.expression, s.bit_width, s.num_vars, t) for s, _f, _e, t in work.items],
-                                        device=device)
-        except (ImportError, AttributeError):
-            path = "plain"
-    step = (lambda: run_batched(work, batcher)) if path == "batched" else (lambda: run_plain(work))
-
-    for _ in range(args.warmup):
-        step()
-    ctx.set_timing(True)
-    with ClockSampler(local) as clocks:
-        ms = timed(step, args.steps, world, device)
-    launch_ms = ctx.launch_times()
-    ctx.set_timing(False)
-    ms_step = max_over_ranks(ms / args.steps, world)
+    ms_step, launch_ms, clocks = measure(path, args.steps)
     value = world * STREAM_COUNT / (ms_step / 1e3)
+    other = "plain" if path == "batched" else "batched"
+    ms_other, launch_other, _clk = measure(other, max(1, min(args.steps, 3)))
+    if path == "batched":
+        ms_plain, plain_launch_ms = ms_other, launch_other
+    else:
+        ms_plain, plain_launch_ms = ms_step, launch_ms
 
-    # roofline of the dominant kernel class, from the launches of the timed region
+    # roofline of the dominant kernel class: algorithmic work per launch over CUDA-event
+    # durations. Batched: the tick times of the last run of the timed region (events inside
+    # the graph); plain: every launch of its timed region.
     per_class = {}
-    launches = []
+
+    def add(L, ms, b, im, launches=1):
+        c = per_class.setdefault(L, {"ms": 0.0, "bytes": 0, "imad": 0, "launches": 0})
+        c["ms"] += ms
+        c["bytes"] += b
+        c["imad"] += im
+        c["launches"] += launches
+
+    work_per_round = []
     for s, spec, _e, _t in work.items:
         enc = s.encoded()
         M = roofline.products_per_point(s.expression)
-        for j in range(s.num_vars):
-            launches.append((spec.limbs, roofline.launch_bytes(enc.num_vars, spec.limbs, s.num_vars, j),
-                             roofline.launch_imad(enc.num_vars, spec.limbs, enc.degree, M, s.num_vars, j)))
-    if path == "plain" and len(launch_ms) == len(launches) * args.steps:
+        work_per_round.append([(spec.limbs, roofline.launch_bytes(enc.num_vars, spec.limbs, s.num_vars, j),
+                                roofline.launch_imad(enc.num_vars, spec.limbs, enc.degree, M, s.num_vars, j))
+                               for j in range(s.num_vars)])
+    if path == "batched":
+        for g, ticks in zip(batcher.groups, batcher.tick_times()):
+            for t, tms in enumerate(ticks):
+                b = sum(work_per_round[i][t][1] for i in g.indices if t < len(work_per_round[i]))
+                im = sum(work_per_round[i][t][2] for i in g.indices if t < len(work_per_round[i]))
+                add(g.spec.limbs, tms, b, im)
+        gpu_launches = sum(len(t) for t in batcher.tick_times()) * args.steps
+    else:
+        flat = [w for rounds in work_per_round for w in rounds]
         for i, t in enumerate(launch_ms):
-            L, b, im = launches[i % len(launches)]
-            c = per_class.setdefault(L, {"ms": 0.0, "bytes": 0, "imad": 0, "launches": 0})
-            c["ms"] += t
-            c["bytes"] += b
-            c["imad"] += im
-            c["launches"] += 1
+            L, b, im = flat[i % len(flat)]
+            add(L, t, b, im)
+        gpu_launches = len(launch_ms)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     roof = None
@@ -385,7 +401,10 @@ def main() -> int:
         "config": {"workload": WORKLOAD, "path": path, "proofs_per_step_per_gpu": STREAM_COUNT,
                    "table_bytes_per_gpu": work.table_bytes(),
                    "l2": "inputs larger than L2 (tables total > 126 MB); no flush", "parallelism": f"replicas x{world}"},
-        "gpu_launches": len(launch_ms) if path == "plain" else None,
+        "plain": {"value": world * STREAM_COUNT / (ms_plain / 1e3), "unit": "proofs/s", "ms_per_step": ms_plain,
+                  "path": "one proof at a time (sc_prove per proof)"},
+        "speedup_vs_plain": ms_plain / ms_step if path == "batched" else 1.0,
+        "gpu_launches": gpu_launches,
         "clocks": clocks.summary(),
         "imad_peak_tera_per_s": imad_rate / 1e12,
     }
@@ -393,7 +412,7 @@ def main() -> int:
         line["roofline"] = roof
 
     if rank == 0 and world == 1 and not args.no_e2e:
-        line["e2e"] = e2e_measure(work, args, device)
+        line["e2e"] = e2e_measure(work, args, device, batcher if path == "batched" else None)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
@@ -407,39 +426,52 @@ def main() -> int:
     return 0
 
 
-def e2e_measure(work: Workload, args, device) -> dict:
-    """Host-buffer path: per step, copy every proof's canonical tables from pinned host
-    memory, convert on the device, prove, read the results back."""
+def e2e_measure(work: Workload, args, device, batcher=None) -> dict:
+    """Host-buffer path: per step, every proof's canonical tables go from pinned host memory
+    to the device and are converted to Montgomery form there; the proofs run (batched, or
+    one sc_prove per proof); every proof's results are read back to the host."""
+    import ctypes
+
     import torch
 
-    from zkduel_b200 import api
+    from zkduel_b200 import _lib, api
 
     host = []
     for s, spec, _e, t in work.items:
         canon = api.download_tables(t, spec)
-        h = torch.from_numpy(canon.view("int32")).pin_memory()
-        host.append(h)
+        host.append(torch.from_numpy(canon.view("int32")).pin_memory())
     h2d = sum(h.numel() * 4 for h in host)
+    ctx = api.get_context(device)
+    lib = _lib.load()
 
-    def step():
-        res = []
-        for (s, spec, expr, _t), h in zip(work.items, host):
-            res.append(api.prove_host(h, expr, spec, s.num_vars, "sha3", device=device))
-        return res
+    if batcher is not None:
+        def step():
+            for (s, spec, _e, t), h in zip(work.items, host):
+                t.copy_(h, non_blocking=True)
+                fld = api.get_device_field(spec, ctx.device)
+                K, _L, N = t.shape
+                _lib.check(lib.sc_tables_to_mont(ctx.handle, fld.handle, ctypes.c_void_p(t.data_ptr()),
+                                                 ctypes.c_uint64(N), int(K)), "sc_tables_to_mont")
+            batcher.run()
+            return batcher.results()
+    else:
+        def step():
+            return [api.prove_host(h, e, spec, s.num_vars, "sha3", device=device)
+                    for (s, spec, e, _t), h in zip(work.items, host)]
 
     step()
     torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
     steps = max(1, min(args.steps, 3))
-    d2h = 0
+    t0 = time.perf_counter()
     for _ in range(steps):
         res = step()
     torch.cuda.synchronize(device)
     dt = (time.perf_counter() - t0) / steps
-    for p in res:
-        d2h += p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
+    d2h = sum(p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
+              for p in res)
     return {"value": STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": dt * 1e3, "path": "plain (host buffers)", "steps": steps}
+            "ms_per_step": dt * 1e3, "path": ("batched" if batcher is not None else "plain") + " (host buffers)",
+            "steps": steps, "timer": "host wall clock around synchronised steps"}
 
 
 if __name__ == "__main__":

@@ -148,6 +148,37 @@ int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_ro
              uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
              uint32_t* out_claim0, uint64_t* out_checksum);
 
+/* ---------------------------------------------------------------- batched proving
+ *
+ * A batch holds `count` independent proofs over one field: proof i proves expression
+ * exprs[i] over num_rounds[i] variables on the device tables tables_dev[i] (layout as for
+ * sc_prove; read only; they must stay allocated while the batch exists). Round t of every
+ * proof runs in one persistent launch ("tick") whose blocks pull (proof, tile) items from a
+ * device work queue; the whole batch is one CUDA graph, replayed by every sc_batch_run.
+ * Challenges: SC_CHALLENGE_SHA3 or SC_CHALLENGE_FIXED. threads (32..256, multiple of 32)
+ * and pairs_per_thread (1..64) set the tile (threads x pairs_per_thread pairs per item);
+ * 0 picks the defaults (256, 2). Results are bit-identical to sc_prove of each proof alone.
+ * No counterpart in the reference, which proves one proof at a time
+ * (cuda/src/field_sumcheck.cu:1012-1088; src/zkduel/api.py:26-64). */
+typedef struct sc_batch sc_batch;
+int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
+                    const int32_t* num_rounds, const uint32_t* const* tables_dev,
+                    int challenge_mode, int threads, int pairs_per_thread, sc_batch** out);
+/* Enqueues one run after the work queued on the context's stream (the context's stream
+ * then waits for it). Asynchronous. */
+int sc_batch_run(sc_batch* batch);
+/* Waits for the last run; its results are then readable with sc_batch_result. */
+int sc_batch_wait(sc_batch* batch);
+/* Outputs of proof `index` of the last run, laid out as sc_prove's. */
+int sc_batch_result(sc_batch* batch, int index, uint32_t* out_round_polys,
+                    uint32_t* out_challenges, uint32_t* out_finals, uint32_t* out_claim0,
+                    uint64_t* out_checksum);
+/* Device time of every tick of the last run (ms; CUDA events recorded inside the graph
+ * around each launch), available after sc_batch_wait; only the first `capacity` are
+ * copied, *count is the number of ticks. */
+int sc_batch_tick_times(sc_batch* batch, float* out_ms, int capacity, int* count);
+int sc_batch_destroy(sc_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,245 @@
+// Host-side pieces shared by the C ABI translation units: error reporting, the opaque
+// handle types, scratch buffers, expression and proof-state layout.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sumcheck_b200.h"
+#include "host_field.h"
+#include "prover.cuh"
+#include "tables.cuh"
+
+using namespace sc;
+
+
+namespace sc_host {
+
+inline thread_local std::string g_err;
+
+inline int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define SC_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return fail(SC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kBlock = 256;
+constexpr int kMaxDynSmem = 200 * 1024;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace sc_host
+
+using sc_host::DevBuf;
+
+struct sc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  DevBuf fold_a, fold_b, partials, state;
+  uint32_t* host_state = nullptr;  // pinned staging of the proof state
+  size_t host_state_bytes = 0;
+  // per-launch timing of the round kernels (off by default)
+  bool timing = false;
+  std::vector<cudaEvent_t> events;   // 2 per launch
+  int events_used = 0;
+  std::vector<float> launch_ms;      // durations of the launches since the last read
+};
+
+struct sc_field {
+  HostField hf;
+  FieldConsts consts;        // host copy
+  FieldConsts* dev = nullptr;
+  int device = -1;
+  bool has_inverses = true;
+};
+
+struct sc_expr {
+  int num_vars = 0, num_terms = 0, degree = 0;
+  std::vector<int64_t> coeffs;
+  std::vector<uint32_t> coeff_limbs;  // num_terms x 8 when given
+  std::vector<int32_t> lens, offs, flat;
+};
+
+namespace sc_host {
+
+inline int ensure(sc_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (bytes <= b.bytes) return SC_OK;
+  if (b.p) {
+    SC_CUDA(cudaStreamSynchronize(ctx->stream));
+    SC_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    return fail(SC_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return SC_OK;
+}
+
+// Events bracketing one launch when timing is on (pool grows as needed).
+inline int timing_begin(sc_ctx* ctx, cudaEvent_t* start) {
+  if (!ctx->timing) return SC_OK;
+  while (static_cast<int>(ctx->events.size()) < ctx->events_used + 2) {
+    cudaEvent_t e;
+    SC_CUDA(cudaEventCreate(&e));
+    ctx->events.push_back(e);
+  }
+  *start = ctx->events[ctx->events_used++];
+  SC_CUDA(cudaEventRecord(*start, ctx->stream));
+  return SC_OK;
+}
+
+inline int timing_end(sc_ctx* ctx) {
+  if (!ctx->timing) return SC_OK;
+  SC_CUDA(cudaEventRecord(ctx->events[ctx->events_used++], ctx->stream));
+  return SC_OK;
+}
+
+// After a synchronisation: turn recorded event pairs into durations.
+inline int timing_collect(sc_ctx* ctx) {
+  if (!ctx->timing) return SC_OK;
+  for (int i = 0; i + 1 < ctx->events_used; i += 2) {
+    float ms = 0.f;
+    SC_CUDA(cudaEventElapsedTime(&ms, ctx->events[i], ctx->events[i + 1]));
+    ctx->launch_ms.push_back(ms);
+  }
+  ctx->events_used = 0;
+  return SC_OK;
+}
+
+template <int L>
+inline int set_kernel_attrs() {
+  SC_CUDA(cudaFuncSetAttribute(round_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+  return SC_OK;
+}
+
+// Montgomery image of a small non-negative integer.
+inline void mont_small(const HostField& hf, const uint32_t* r2, uint64_t v, uint32_t* out) {
+  uint32_t w[2] = {static_cast<uint32_t>(v), static_cast<uint32_t>(v >> 32)};
+  uint32_t red[8];
+  hf.reduce(w, 2, red);
+  hf.mul(red, r2, out);
+}
+
+inline void mont_pow(const HostField& hf, const uint32_t* base, const uint32_t* e, const uint32_t* one,
+              uint32_t* out) {
+  uint32_t acc[8];
+  std::memcpy(acc, one, 32);
+  for (int w = hf.L - 1; w >= 0; --w)
+    for (int b = 31; b >= 0; --b) {
+      hf.mul(acc, acc, acc);
+      if ((e[w] >> b) & 1u) hf.mul(acc, base, acc);
+    }
+  std::memcpy(out, acc, 4 * hf.L);
+}
+
+// Checks the CIOS exactness bound: (p - 1) 2^32 + p < 2^(32 (L + 1)).
+inline bool cios_bound_holds(const HostField& hf) {
+  const int L = hf.L;
+  uint32_t x[10] = {0};
+  uint32_t pm1[8];
+  std::memcpy(pm1, hf.p, 4 * L);
+  pm1[0] -= 1;  // p odd, so no borrow
+  for (int i = 0; i < L; ++i) x[i + 1] = pm1[i];
+  uint64_t c = 0;
+  for (int i = 0; i < L + 2; ++i) {
+    uint64_t s = static_cast<uint64_t>(x[i]) + (i < L ? hf.p[i] : 0u) + c;
+    x[i] = static_cast<uint32_t>(s);
+    c = s >> 32;
+  }
+  return x[L + 1] == 0 && c == 0;
+}
+
+template <int L>
+inline void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
+  std::memset(&E, 0, sizeof(E));
+  E.num_vars = ex.num_vars;
+  E.num_terms = ex.num_terms;
+  E.degree = ex.degree;
+  const HostField& hf = f.hf;
+  const int mul_cost = 4 * L * L + 8 * L, add_cost = 3 * L + 3;
+  for (int i = 0; i < ex.num_terms; ++i) {
+    E.term_len[i] = static_cast<uint8_t>(ex.lens[i]);
+    E.term_off[i] = static_cast<uint8_t>(ex.offs[i]);
+    bool use_mont = !ex.coeff_limbs.empty();
+    const int64_t c = ex.coeffs[i];
+    if (!use_mont) {
+      if (c == 1) {
+        E.coeff_kind[i] = kCoeffPlus;
+      } else if (c == -1) {
+        E.coeff_kind[i] = kCoeffMinus;
+      } else if (c > -(int64_t{1} << 31) && c < (int64_t{1} << 31)) {
+        const uint64_t m = c < 0 ? static_cast<uint64_t>(-c) : static_cast<uint64_t>(c);
+        const int bits = m ? 64 - __builtin_clzll(m) : 0;
+        const int chain = (bits > 0 ? bits - 1 : 0) + (m ? __builtin_popcountll(m) - 1 : 0) + (c < 0);
+        if (chain * add_cost <= mul_cost) {
+          E.coeff_kind[i] = kCoeffSmall;
+          E.coeff_small[i] = static_cast<int32_t>(c);
+        } else {
+          use_mont = true;
+        }
+      } else {
+        use_mont = true;
+      }
+    }
+    if (use_mont) {
+      E.coeff_kind[i] = kCoeffMont;
+      uint32_t red[8];
+      if (!ex.coeff_limbs.empty()) {
+        hf.reduce(&ex.coeff_limbs[8 * i], 8, red);
+      } else {
+        const uint64_t m = c < 0 ? static_cast<uint64_t>(-(c + 1)) + 1u : static_cast<uint64_t>(c);
+        uint32_t w[2] = {static_cast<uint32_t>(m), static_cast<uint32_t>(m >> 32)};
+        hf.reduce(w, 2, red);
+        if (c < 0) hf.neg(red, red);
+      }
+      uint32_t mont[8];
+      hf.mul(red, f.consts.r2, mont);
+      for (int l = 0; l < L; ++l) E.coeff_mont[i][l] = mont[l];
+    }
+  }
+  for (size_t i = 0; i < ex.flat.size(); ++i) E.flat[i] = static_cast<uint8_t>(ex.flat[i]);
+}
+
+struct StateOffsets {
+  size_t counter, status, checksum, polys, chals, finals, claim0, total_words;
+};
+
+inline StateOffsets state_offsets(int n, int K, int L) {
+  StateOffsets o;
+  o.counter = 0;
+  o.status = 1;
+  o.checksum = 2;  // u64 at word 2 (8-byte aligned)
+  o.polys = 4;
+  o.chals = o.polys + static_cast<size_t>(n) * kMaxPoints * L;
+  o.finals = o.chals + static_cast<size_t>(n) * L;
+  o.claim0 = o.finals + static_cast<size_t>(1 + K) * L;
+  o.total_words = o.claim0 + L;
+  return o;
+}
+
+}  // namespace sc_host

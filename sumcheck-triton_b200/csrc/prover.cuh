@@ -284,57 +284,41 @@ __device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const Field
 // Dynamic shared memory per thread: values and differences of every table.
 __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { return 2 * K * L; }
 
+// Folds (if A.fold) and evaluates pairs q = first, first + stride, ... < last, adding the
+// d+1 point sums into acc. sv / sd: this block's [K][L][nthr] shared arrays.
 template <int L>
-__global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const ExprDev E,
-                                                    const FieldParams<L> F) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
-  __shared__ __align__(16) uint8_t msg[3 * 136];
-  __shared__ int is_last;
-
-  const int tid = threadIdx.x;
-  const int nthr = blockDim.x;
-  const int K = E.num_vars;
-  const int d = E.degree;
-  uint32_t* sv = smem;              // [K][L][nthr] values at the current point
-  uint32_t* sd = smem + K * L * nthr;  // [K][L][nthr] differences o - e
-
-  Fe<L> acc[kMaxPoints];
-#pragma unroll
-  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
-
-  Fe<L> r_prev = fe_zero<L>();
-  if (A.fold) r_prev = ld_fe_cg<L>(A.st.chals + (A.round - 1) * L);
-
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * nthr;
-  for (uint64_t q = static_cast<uint64_t>(blockIdx.x) * nthr + tid; q < A.pairs; q += stride) {
-    // load (and fold) the pair of every table
+__device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst, uint64_t src_len, bool fold,
+                                              const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
+                                              uint64_t first, uint64_t last, uint64_t stride,
+                                              Fe<L> (&acc)[kMaxPoints], const FieldParams<L>& F) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int K = E.num_vars, d = E.degree;
+  for (uint64_t q = first; q < last; q += stride) {
     for (int k = 0; k < K; ++k) {
       Fe<L> e, o;
-      if (A.fold) {
+      if (fold) {
         Fe<L> x0, x1, x2, x3;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-          const uint4 v = __ldcs(reinterpret_cast<const uint4*>(A.src + (static_cast<uint64_t>(k) * L + l) * A.src_len) + q);
+          const uint4 v = __ldcs(reinterpret_cast<const uint4*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
           x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
         }
         e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
         o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
-        const uint64_t dst_len = A.src_len >> 1;
+        const uint64_t dst_len = src_len >> 1;
 #pragma unroll
         for (int l = 0; l < L; ++l)
-          reinterpret_cast<uint2*>(A.dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+          reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
       } else {
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-          const uint2 v = __ldcs(reinterpret_cast<const uint2*>(A.src + (static_cast<uint64_t>(k) * L + l) * A.src_len) + q);
+          const uint2 v = __ldcs(reinterpret_cast<const uint2*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
           e.w[l] = v.x; o.w[l] = v.y;
         }
       }
       sm_put<L>(sv, k, tid, nthr, e);
       sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
     }
-    // extend to t = 0..d and evaluate
 #pragma unroll
     for (int t = 0; t < kMaxPoints; ++t) {
       if (t > d) break;
@@ -345,6 +329,48 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
       acc[t] = fe_add(acc[t], eval_expr<L>(E, sv, tid, nthr, F), F);
     }
   }
+}
+
+// Sums the partials of blocks/items [first, first + count) into g_sm[t * L + l] (block-wide).
+template <int L>
+__device__ __forceinline__ void reduce_partials(const uint32_t* partials, uint64_t first, uint64_t count, int d,
+                                                uint32_t* scratch, uint32_t* g_sm, const FieldParams<L>& F) {
+  Fe<L> acc[kMaxPoints];
+#pragma unroll
+  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+  for (uint64_t b = threadIdx.x; b < count; b += blockDim.x) {
+    const uint32_t* pb = partials + (first + b) * kMaxPoints * L;
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) {
+      if (t > d) break;
+      acc[t] = fe_add(acc[t], ld_fe_cg<L>(pb + t * L), F);
+    }
+  }
+  block_reduce<L>(acc, d, scratch, g_sm, F);
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const ExprDev E,
+                                                    const FieldParams<L> F) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
+  __shared__ __align__(16) uint8_t msg[3 * 136];
+  __shared__ int is_last;
+
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int d = E.degree;
+  uint32_t* sv = smem;                           // [K][L][nthr] values at the current point
+  uint32_t* sd = smem + E.num_vars * L * nthr;   // [K][L][nthr] differences o - e
+
+  Fe<L> acc[kMaxPoints];
+#pragma unroll
+  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+  Fe<L> r_prev = fe_zero<L>();
+  if (A.fold) r_prev = ld_fe_cg<L>(A.st.chals + (A.round - 1) * L);
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * nthr;
+  process_pairs<L>(A.src, A.dst, A.src_len, A.fold != 0, r_prev, E, sv, sd,
+                   static_cast<uint64_t>(blockIdx.x) * nthr + tid, A.pairs, stride, acc, F);
 
   // block partial -> global; the last block reduces all partials
   __syncthreads();
@@ -356,22 +382,101 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-
-#pragma unroll
-  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
-  for (uint32_t b = tid; b < gridDim.x; b += nthr) {
-    const uint32_t* pb = A.partials + static_cast<uint64_t>(b) * kMaxPoints * L;
-#pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) {
-      if (t > d) break;
-      acc[t] = fe_add(acc[t], ld_fe_cg<L>(pb + t * L), F);
-    }
-  }
-  block_reduce<L>(acc, d, smem, g_sm, F);
+  reduce_partials<L>(A.partials, 0, gridDim.x, d, smem, g_sm, F);
   if (tid < 32) finalize_round<L>(A, E, F, g_sm, msg);
   if (tid == 0) {
     __threadfence();
     *A.st.counter = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------ batched
+//
+// Many independent proofs advance one round per "tick". A tick is one launch per field
+// class: a persistent kernel whose blocks pull (proof round, tile of pairs) items from a
+// device work queue (an atomic counter over the tick's item list). Every item leaves one
+// partial; the block that finishes the last item of a proof's round (per-proof atomic
+// ticket) reduces that proof's partials and finalises its round -- SHA3 challenge
+// included -- while the other blocks go on with other proofs' items.
+
+struct BatchRound {
+  RoundArgs args;      // this proof's round (src/dst/len/pairs/round/fold/mode/fc/state)
+  int32_t expr;        // index into the batch's expression table
+  int32_t first_item;  // this round's items: [first_item, first_item + num_items)
+  int32_t num_items;
+  int32_t pad;
+};
+
+struct BatchItem {
+  int32_t round;       // index into the tick's BatchRound array
+  int32_t pad;
+  uint64_t start;      // pairs [start, start + count)
+  uint64_t count;
+};
+
+struct BatchTickArgs {
+  const BatchRound* rounds;
+  const BatchItem* items;
+  int32_t num_items;
+  int32_t pad;
+  uint32_t* head;      // queue counter of this tick (zero before the launch)
+  const ExprDev* exprs;
+  uint32_t* partials;  // [num_items][kMaxPoints][L], indexed by item
+};
+
+template <int L>
+__global__ void __launch_bounds__(256) batch_round_kernel(const BatchTickArgs T, const FieldParams<L> F) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
+  __shared__ __align__(16) uint8_t msg[3 * 136];
+  __shared__ __align__(16) ExprDev E;
+  __shared__ __align__(16) BatchRound R;
+  __shared__ int item_sm, is_last, cur_expr;
+
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  if (tid == 0) cur_expr = -1;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) item_sm = static_cast<int>(atomicAdd(T.head, 1u));
+    __syncthreads();
+    const int it = item_sm;
+    if (it >= T.num_items) break;
+    const BatchItem I = T.items[it];
+    if (tid == 0) R = T.rounds[I.round];
+    __syncthreads();
+    if (R.expr != cur_expr) {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(T.exprs + R.expr);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&E);
+      for (int i = tid; i < static_cast<int>(sizeof(ExprDev) / 4); i += nthr) dst[i] = src[i];
+      __syncthreads();
+      if (tid == 0) cur_expr = R.expr;
+    }
+    const int d = E.degree;
+    Fe<L> acc[kMaxPoints];
+#pragma unroll
+    for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+    Fe<L> r_prev = fe_zero<L>();
+    if (R.args.fold) r_prev = ld_fe_cg<L>(R.args.st.chals + (R.args.round - 1) * L);
+    uint32_t* sv = smem;
+    uint32_t* sd = smem + E.num_vars * L * nthr;
+    process_pairs<L>(R.args.src, R.args.dst, R.args.src_len, R.args.fold != 0, r_prev, E, sv, sd,
+                     I.start + tid, I.start + I.count, nthr, acc, F);
+    __syncthreads();
+    block_reduce<L>(acc, d, smem, g_sm, F);
+    if (tid < (d + 1) * L) T.partials[static_cast<uint64_t>(it) * kMaxPoints * L + tid] = g_sm[tid];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.num_items - 1));
+    __syncthreads();
+    if (is_last) {
+      __threadfence();
+      reduce_partials<L>(T.partials, R.first_item, R.num_items, d, smem, g_sm, F);
+      if (tid < 32) finalize_round<L>(R.args, E, F, g_sm, msg);
+      if (tid == 0) {
+        __threadfence();
+        *R.args.st.counter = 0;
+      }
+    }
   }
 }
 

@@ -140,7 +140,7 @@ __global__ void field_apply_kernel(int op, const uint32_t* a, const uint32_t* b,
 // Integer multiply-add throughput probe: every thread runs 8 independent chains of
 // mad.lo / mad.hi (the instruction pair of the Montgomery product), so the count of
 // multiply-adds is exact: iters x 8 chains x 2 per thread.
-__global__ void imad_probe_kernel(uint32_t* sink, int iters, uint32_t seed) {
+static __global__ void imad_probe_kernel(uint32_t* sink, int iters, uint32_t seed) {
   uint32_t a[8], b[8];
   const uint32_t x = seed ^ threadIdx.x, y = seed * 0x9E3779B9u + blockIdx.x;
 #pragma unroll

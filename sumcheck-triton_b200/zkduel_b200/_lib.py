@@ -57,6 +57,16 @@ SIGNATURES = {
     "sc_tables_to_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_tables_from_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_field_apply": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_uint64]),
+    "sc_batch_create": (
+        c_int,
+        [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_int32), POINTER(c_void_p), c_int, c_int, c_int,
+         POINTER(c_void_p)],
+    ),
+    "sc_batch_run": (c_int, [c_void_p]),
+    "sc_batch_wait": (c_int, [c_void_p]),
+    "sc_batch_result": (c_int, [c_void_p, c_int, U32P, U32P, U32P, U32P, U64P]),
+    "sc_batch_tick_times": (c_int, [c_void_p, POINTER(c_float), c_int, POINTER(c_int)]),
+    "sc_batch_destroy": (c_int, [c_void_p]),
     "sc_calibrate_imad": (c_int, [c_void_p, POINTER(c_double)]),
     "sc_prove": (
         c_int,

@@ -1,0 +1,139 @@
+"""Batched proving: many independent proofs in one CUDA graph per field.
+
+``BatchProver`` groups the proofs by field (modulus and limb count) and builds one native
+batch (``sc_batch_create``) per group. Each batch runs on its own stream, so the groups
+overlap on the device (a 64-bit group is memory-bound, a 256-bit group multiply-bound).
+Within a group, round t of every proof runs in one persistent launch whose blocks pull
+(proof, tile) items from a device work queue; the whole group is one CUDA graph.
+
+Results are bit-identical to proving each proof alone (``prove_device``); the tests check
+exactly that.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from .api import CompiledExpression, Proof, get_context, get_device_field
+from .expression import encode_expression
+from .fields import FieldSpec, get_field
+
+
+@dataclass
+class _Group:
+    spec: FieldSpec
+    indices: list[int]
+    exprs: list[CompiledExpression]
+    handle: ctypes.c_void_p
+
+
+class BatchProver:
+    """Proves ``items`` = [(expression, bit_width, num_vars, tables), ...] together.
+
+    ``tables`` are device tensors (K, L, 2^n) of Montgomery limbs (``generate_tables`` /
+    ``upload_tables``); they must stay alive while the prover exists.
+    ``tile`` maps a limb count to (threads per block, pairs per thread); None = defaults.
+    """
+
+    def __init__(self, items: Sequence[tuple], device=None, challenge_mode: str = "sha3",
+                 tile: dict[int, tuple[int, int]] | None = None, fields: Sequence[FieldSpec] | None = None):
+        lib = _lib.load()
+        self.ctx = get_context(device)
+        self.items = list(items)
+        mode = _lib.CHALLENGE_MODES[challenge_mode]
+        if mode == _lib.SC_CHALLENGE_EXPLICIT:
+            raise ValueError("batches derive their challenges: 'sha3' or 'fixed'")
+        self.mode = challenge_mode
+        specs = list(fields) if fields is not None else [get_field(bw) for _e, bw, _n, _t in self.items]
+        groups: dict[tuple[int, int], list[int]] = {}
+        for i, spec in enumerate(specs):
+            groups.setdefault((spec.modulus, spec.limbs), []).append(i)
+        self.groups: list[_Group] = []
+        self._keep = []
+        for (_q, L), idx in groups.items():
+            spec = specs[idx[0]]
+            fld = get_device_field(spec, self.ctx.device)
+            exprs = []
+            for i in idx:
+                e = self.items[i][0]
+                exprs.append(e if isinstance(e, CompiledExpression) else CompiledExpression(encode_expression(e), spec.modulus))
+            n = len(idx)
+            expr_arr = (ctypes.c_void_p * n)(*[e.handle.value for e in exprs])
+            rounds = (ctypes.c_int32 * n)(*[int(self.items[i][2]) for i in idx])
+            tabs = (ctypes.c_void_p * n)(*[self.items[i][3].data_ptr() for i in idx])
+            for i, e in zip(idx, exprs):
+                t = self.items[i][3]
+                want = (e.num_vars, L, 1 << int(self.items[i][2]))
+                if tuple(t.shape) != want or not t.is_contiguous():
+                    raise ValueError(f"proof {i}: tables {tuple(t.shape)}, expected contiguous {want}")
+            threads, ppt = (tile or {}).get(L, (0, 0))
+            h = ctypes.c_void_p()
+            rc = lib.sc_batch_create(self.ctx.handle, fld.handle, n, expr_arr, rounds, tabs, mode,
+                                     int(threads), int(ppt), ctypes.byref(h))
+            _lib.check(rc, "sc_batch_create")
+            self.groups.append(_Group(spec, idx, exprs, h))
+            self._keep.append((expr_arr, rounds, tabs))
+
+    def launch(self) -> None:
+        """Enqueues one run of every group (asynchronous)."""
+        lib = _lib.load()
+        for g in self.groups:
+            _lib.check(lib.sc_batch_run(g.handle), "sc_batch_run")
+
+    def wait(self) -> None:
+        lib = _lib.load()
+        for g in self.groups:
+            _lib.check(lib.sc_batch_wait(g.handle), "sc_batch_wait")
+
+    def run(self) -> None:
+        self.launch()
+        self.wait()
+
+    def tick_times(self) -> list[list[float]]:
+        out = []
+        lib = _lib.load()
+        for g in self.groups:
+            cnt = ctypes.c_int(0)
+            _lib.check(lib.sc_batch_tick_times(g.handle, None, 0, ctypes.byref(cnt)), "sc_batch_tick_times")
+            buf = (ctypes.c_float * max(1, cnt.value))()
+            _lib.check(lib.sc_batch_tick_times(g.handle, buf, cnt.value, ctypes.byref(cnt)), "sc_batch_tick_times")
+            out.append(list(buf)[: cnt.value])
+        return out
+
+    def result(self, i: int) -> Proof:
+        """Outputs of proof ``i`` of the last run."""
+        for g in self.groups:
+            if i in g.indices:
+                j = g.indices.index(i)
+                e = g.exprs[j]
+                L, n, d, K = g.spec.limbs, int(self.items[i][2]), e.degree, e.num_vars
+                polys = np.zeros((n, d + 1, L), dtype=np.uint32)
+                chals = np.zeros((n, L), dtype=np.uint32)
+                finals = np.zeros((1 + K, L), dtype=np.uint32)
+                claim0 = np.zeros((L,), dtype=np.uint32)
+                cs = ctypes.c_uint64(0)
+                p = lambda a: a.ctypes.data_as(_lib.U32P)  # noqa: E731
+                rc = _lib.load().sc_batch_result(g.handle, j, p(polys), p(chals), p(finals), p(claim0), ctypes.byref(cs))
+                _lib.check(rc, "sc_batch_result")
+                return Proof(g.spec, n, d, e.encoded.var_names, polys, chals, finals, claim0, int(cs.value))
+        raise IndexError(i)
+
+    def results(self) -> list[Proof]:
+        return [self.result(i) for i in range(len(self.items))]
+
+    def close(self) -> None:
+        for g in self.groups:
+            if g.handle:
+                _lib.load().sc_batch_destroy(g.handle)
+                g.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,93 @@
+"""Batched proving (GPU): every proof of a batch equals the same proof proved alone."""
+
+from __future__ import annotations
+
+import random
+
+import numpy as np
+import pytest
+
+from helpers import assert_proof_equals_oracle, oracle_tables
+from oracle import oracle as O
+from zkduel_b200 import api
+from zkduel_b200.batch import BatchProver
+from zkduel_b200.fields import get_field
+from zkduel_b200.streams import batched_stream
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a GPU", allow_module_level=True)
+
+
+def _tables(spec, s):
+    return api.generate_tables(spec, s.num_tables, s.num_vars, [0] * s.num_tables, s.seed)
+
+
+def _same(a, b):
+    assert np.array_equal(a.round_polys_mont, b.round_polys_mont)
+    assert np.array_equal(a.challenges_mont, b.challenges_mont)
+    assert np.array_equal(a.finals_mont, b.finals_mont)
+    assert np.array_equal(a.claim0_mont, b.claim0_mont)
+    assert a.checksum == b.checksum
+
+
+def _mixed(count, lo, hi, seed):
+    rng = random.Random(seed)
+    out = []
+    for s in batched_stream(count, seed):
+        n = rng.randint(lo, hi)
+        out.append(type(s)(s.index, s.bit_width, n, s.seed, s.expression))
+    return out
+
+
+@pytest.mark.parametrize("tile", [None, {2: (64, 1), 8: (32, 1)}, {2: (256, 8), 8: (128, 4)}])
+def test_small_mixed_batch_equals_single_proofs(tile):
+    specs = _mixed(40, 1, 12, 7)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    bp = BatchProver(items, tile=tile)
+    bp.run()
+    for i, s in enumerate(specs):
+        spec = get_field(s.bit_width)
+        alone = api.prove_device(items[i][3], s.expression, spec, s.num_vars, "sha3")
+        _same(bp.result(i), alone)
+
+
+def test_batch_matches_oracle():
+    specs = _mixed(6, 2, 6, 3)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    bp = BatchProver(items)
+    bp.run()
+    for i, s in enumerate(specs):
+        spec = get_field(s.bit_width)
+        terms, k = O.indexed_terms(s.expression)
+        res = O.prove(terms, k, spec.modulus, spec.limbs, oracle_tables(["uniform"] * k, s.seed, s.num_vars, spec), "sha3")
+        assert_proof_equals_oracle(bp.result(i), res, spec)
+
+
+def test_stream_batch_replays_identically():
+    specs = batched_stream(48, 11)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    bp = BatchProver(items)
+    bp.run()
+    first = bp.results()
+    bp.run()
+    for a, b in zip(first, bp.results()):
+        _same(a, b)
+    for i in (0, 7, 23, 47):
+        s = specs[i]
+        _same(first[i], api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
+    times = bp.tick_times()
+    assert len(times) == 2 and all(len(t) == max(specs[i].num_vars for i in g.indices) for t, g in zip(times, bp.groups))
+    assert all(x > 0 for t in times for x in t)
+
+
+def test_fixed_mode_and_rejects_explicit():
+    specs = _mixed(5, 3, 5, 1)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    bp = BatchProver(items, challenge_mode="fixed")
+    bp.run()
+    for i, s in enumerate(specs):
+        _same(bp.result(i), api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "fixed"))
+    with pytest.raises(ValueError):
+        BatchProver(items, challenge_mode="explicit")
