@@ -173,10 +173,10 @@ int batch_issue(sc_batch* B) {
     T.exprs = static_cast<const ExprDev*>(B->exprs.p);
     T.partials = static_cast<uint32_t*>(B->partials.p) + static_cast<size_t>(B->tick_item0[t]) * kMaxPoints * L;
     const unsigned grid = static_cast<unsigned>(std::min(B->grid, std::max(1, T.num_items)));
-    SC_CUDA(cudaEventRecord(B->tick_events[2 * t], B->stream));
+    SC_CUDA(cudaEventRecordWithFlags(B->tick_events[2 * t], B->stream, cudaEventRecordExternal));
     batch_round_kernel<L><<<grid, B->threads, B->smem, B->stream>>>(T, F);
     SC_CUDA(cudaGetLastError());
-    SC_CUDA(cudaEventRecord(B->tick_events[2 * t + 1], B->stream));
+    SC_CUDA(cudaEventRecordWithFlags(B->tick_events[2 * t + 1], B->stream, cudaEventRecordExternal));
   }
   SC_CUDA(cudaMemcpyAsync(B->host_state, B->state.p, B->state_words * 4, cudaMemcpyDeviceToHost, B->stream));
   return SC_OK;

@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
   // block partial -> global; the last block reduces all partials
   __syncthreads();
   block_reduce<L>(acc, d, smem, g_sm, F);
-  if (tid < (d + 1) * L) A.partials[static_cast<uint64_t>(blockIdx.x) * kMaxPoints * L + tid] = g_sm[tid];
+  for (int i = tid; i < (d + 1) * L; i += nthr) A.partials[static_cast<uint64_t>(blockIdx.x) * kMaxPoints * L + i] = g_sm[i];
   __threadfence();
   __syncthreads();
   if (tid == 0) is_last = (atomicAdd(A.st.counter, 1u) == gridDim.x - 1);
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(256) batch_round_kernel(const BatchTickArgs T,
                      I.start + tid, I.start + I.count, nthr, acc, F);
     __syncthreads();
     block_reduce<L>(acc, d, smem, g_sm, F);
-    if (tid < (d + 1) * L) T.partials[static_cast<uint64_t>(it) * kMaxPoints * L + tid] = g_sm[tid];
+    for (int i = tid; i < (d + 1) * L; i += nthr) T.partials[static_cast<uint64_t>(it) * kMaxPoints * L + i] = g_sm[i];
     __threadfence();
     __syncthreads();
     if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.num_items - 1));
