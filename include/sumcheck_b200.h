@@ -148,6 +148,22 @@ int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_ro
              uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
              uint32_t* out_claim0, uint64_t* out_checksum);
 
+/* sc_prove without any allocation, for callers that cannot call cudaMalloc (code inside
+ * another framework's memory pool or under a fixed device-memory budget, plug-ins that may
+ * not grow the process's footprint after start-up). No counterpart in the reference.
+ * Same arguments and outputs as sc_prove (outputs are written straight into the caller's
+ * host arrays). Its scratch is one 32 MiB array in device memory that every GPU loading
+ * the library holds until exit; proofs needing more (about K L 2^n 3 bytes of fold
+ * buffers plus under 1 MiB) fail with SC_ERR_UNSUPPORTED before anything runs. The first
+ * call on a device looks up that array's device address: make it before any stream
+ * capture. Calls share the array: calls that overlap on one GPU race, so issue them on
+ * one stream or one after another. */
+int sc_prove_noalloc(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,
+                     const uint32_t* tables_dev, int challenge_mode,
+                     const uint32_t* explicit_challenges, uint32_t* out_round_polys,
+                     uint32_t* out_challenges, uint32_t* out_finals, uint32_t* out_claim0,
+                     uint64_t* out_checksum);
+
 /* ---------------------------------------------------------------- batched proving
  *
  * A batch holds `count` independent proofs over one field: proof i proves expression

@@ -33,7 +33,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     hdr = CSRC / "field_ptx.cuh"
     if _stale(hdr, [gen]):
         subprocess.check_call([sys.executable, str(gen)])
-    sources = [CSRC / "capi.cu", CSRC / "batch.cu"]
+    sources = [CSRC / "capi.cu", CSRC / "batch.cu", CSRC / "noalloc.cu"]
     deps = sources + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "sumcheck_b200.h"]
     if not force and not _stale(LIB, deps):
         return LIB

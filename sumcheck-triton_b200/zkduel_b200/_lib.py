@@ -57,6 +57,10 @@ SIGNATURES = {
     "sc_tables_to_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_tables_from_mont": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int]),
     "sc_field_apply": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_uint64]),
+    "sc_prove_noalloc": (
+        c_int,
+        [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, U32P, U32P, U32P, U32P, U32P, U64P],
+    ),
     "sc_batch_create": (
         c_int,
         [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_int32), POINTER(c_void_p), c_int, c_int, c_int,
