@@ -56,7 +56,26 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="profile mode: prove one plain config (plain_p32|plain_goldilocks|plain_bls) twice and exit")
     ap.add_argument("--case-vars", type=int, default=None, help="num_vars for --case (default: the config's)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="profile mode: build the mixed stream (--stream-count proofs), run the batch twice, exit")
+    ap.add_argument("--stream-count", type=int, default=STREAM_COUNT, help="proofs in the stream (profile mode)")
     return ap.parse_args()
+
+
+def profile_batch(args) -> int:
+    """The batched path on a (smaller) mixed stream, twice; for ncu captures."""
+    import torch
+
+    from zkduel_b200.batch import BatchProver
+
+    work = Workload(master_seed=0, device=torch.device("cuda", 0), count=args.stream_count)
+    bp = BatchProver([(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items])
+    for _ in range(2):
+        bp.run()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_batch": args.stream_count, "table_bytes": work.table_bytes(),
+                      "checksum0": bp.result(0).checksum}))
+    return 0
 
 
 def profile_case(args) -> int:
@@ -192,14 +211,14 @@ def max_over_ranks(x: float, world: int) -> float:
 class Workload:
     """The stream's proofs with their tables resident on the device."""
 
-    def __init__(self, master_seed: int, device):
+    def __init__(self, master_seed: int, device, count: int = STREAM_COUNT):
         import torch
 
         from zkduel_b200 import api
         from zkduel_b200.fields import get_field
         from zkduel_b200.streams import batched_stream
 
-        self.specs = batched_stream(STREAM_COUNT, master_seed)
+        self.specs = batched_stream(count, master_seed)
         self.items = []
         for s in self.specs:
             spec = get_field(s.bit_width)
@@ -300,6 +319,8 @@ def main() -> int:
     args = parse()
     if args.case:
         return profile_case(args)
+    if args.profile_batch:
+        return profile_batch(args)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -362,12 +383,29 @@ def main() -> int:
                                 roofline.launch_imad(enc.num_vars, spec.limbs, enc.degree, M, s.num_vars, j))
                                for j in range(s.num_vars)])
     if path == "batched":
-        for g, ticks in zip(batcher.groups, batcher.tick_times()):
-            for t, tms in enumerate(ticks):
-                b = sum(work_per_round[i][t][1] for i in g.indices if t < len(work_per_round[i]))
-                im = sum(work_per_round[i][t][2] for i in g.indices if t < len(work_per_round[i]))
-                add(g.spec.limbs, tms, b, im)
-        gpu_launches = sum(len(t) for t in batcher.tick_times()) * args.steps
+        # Degree classes of one field run concurrently on their own streams: a field's
+        # kernel time is the union of its ticks' [start, end] intervals (busy time).
+        classes = batcher.tick_times()
+        spans = {}
+        for c in classes:
+            for t, (a, b_) in enumerate(zip(c["start"], c["end"])):
+                b = sum(work_per_round[i][t][1] for i in c["proofs"] if t < len(work_per_round[i]))
+                im = sum(work_per_round[i][t][2] for i in c["proofs"] if t < len(work_per_round[i]))
+                add(c["limbs"], 0.0, b, im)
+                spans.setdefault(c["limbs"], []).append((a, b_))
+        for L, iv in spans.items():
+            iv.sort()
+            busy, cur_a, cur_b = 0.0, None, None
+            for a, b_ in iv:
+                if cur_b is None or a > cur_b:
+                    if cur_b is not None:
+                        busy += cur_b - cur_a
+                    cur_a, cur_b = a, b_
+                else:
+                    cur_b = max(cur_b, b_)
+            busy += cur_b - cur_a
+            per_class[L]["ms"] = busy
+        gpu_launches = sum(len(c["ms"]) for c in classes) * args.steps
     else:
         flat = [w for rounds in work_per_round for w in rounds]
         for i, t in enumerate(launch_ms):
@@ -382,15 +420,17 @@ def main() -> int:
         if L >= 4:
             ach = c["imad"] / (c["ms"] / 1e3) / 1e12
             pk = imad_rate / 1e12
-            roof = {"bound": "imad", "kernel": f"round_kernel<{L}>", "achieved": ach, "peak": pk,
+            kname = f"batch_round_kernel<{L}, *, *>" if path == "batched" else f"round_kernel<{L}, *, *>"
+            roof = {"bound": "imad", "kernel": kname, "achieved": ach, "peak": pk,
                     "unit": "TIMAD/s", "frac": ach / pk, "traffic": None,
                     "peak_source": "sc_calibrate_imad probe (measured live)"}
         else:
             ach = c["bytes"] / (c["ms"] / 1e3) / 1e9
-            roof = {"bound": "hbm", "kernel": f"round_kernel<{L}>", "achieved": ach, "peak": hbm_peak,
+            kname = f"batch_round_kernel<{L}, *, *>" if path == "batched" else f"round_kernel<{L}, *, *>"
+            roof = {"bound": "hbm", "kernel": kname, "achieved": ach, "peak": hbm_peak,
                     "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None,
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
-        roof["by_class"] = {f"L{k}": {"ms": v["ms"], "launches": v["launches"],
+        roof["by_class"] = {f"L{k}": {"busy_ms": v["ms"], "launches": v["launches"],
                                       "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                       "TIMAD/s": v["imad"] / (v["ms"] / 1e3) / 1e12} for k, v in per_class.items()}
 

@@ -189,10 +189,18 @@ int sc_batch_wait(sc_batch* batch);
 int sc_batch_result(sc_batch* batch, int index, uint32_t* out_round_polys,
                     uint32_t* out_challenges, uint32_t* out_finals, uint32_t* out_claim0,
                     uint64_t* out_checksum);
-/* Device time of every tick of the last run (ms; CUDA events recorded inside the graph
- * around each launch), available after sc_batch_wait; only the first `capacity` are
- * copied, *count is the number of ticks. */
-int sc_batch_tick_times(sc_batch* batch, float* out_ms, int capacity, int* count);
+/* A batch splits its proofs by degree class (degree <= 2, <= 4, <= 7); each class runs
+ * its own sequence of ticks on its own stream. sc_batch_classes gives each class's degree
+ * bound and tick count; sc_batch_class_proofs the indices of its proofs. */
+int sc_batch_classes(sc_batch* batch, int32_t* out_degree_class, int32_t* out_ticks, int capacity,
+                     int* count);
+int sc_batch_class_proofs(sc_batch* batch, int cls, int32_t* out_indices, int capacity, int* count);
+/* Start and end of every tick of the last run, in ms from the run's start (CUDA events
+ * recorded inside the graph around each launch), class after class in sc_batch_classes
+ * order, available after sc_batch_wait. Classes overlap in time; a kernel's duration is
+ * end - start. Only the first `capacity` are copied; *count is the number of ticks. */
+int sc_batch_tick_times(sc_batch* batch, float* out_start_ms, float* out_end_ms, int capacity,
+                        int* count);
 int sc_batch_destroy(sc_batch* batch);
 
 #ifdef __cplusplus

@@ -1,12 +1,14 @@
 // Batched proving: many independent proofs of one field in one CUDA graph.
 //
-// Proof p (num_rounds n_p) does its round t in tick t. A tick is one launch of
-// batch_round_kernel<L> over a work queue of (proof round, tile) items built here on the
-// host: a round of P pairs is cut into ceil(P / tile) items, tile = threads x pairs per
-// thread. The whole batch -- state reset, every tick, the copy of all proof states to
-// pinned host memory -- is captured once into a CUDA graph on the batch's own stream and
-// replayed by every sc_batch_run. The reference has no batching (every proof runs alone,
-// with a blocking copy per interpolation point: cuda/src/field_sumcheck.cu:1012-1088).
+// Proof p (num_rounds n_p) does its round t in tick t. The proofs of a batch are split by
+// degree class (the kernel's register arrays are sized by the class), and every class runs
+// its own sequence of ticks on its own stream. A tick is one launch of
+// batch_round_kernel<L, K, DMAX> over a work queue of (proof round, tile) items built here on
+// the host: a round of P pairs is cut into ceil(P / tile) items, tile = threads x pairs per
+// thread. The whole batch -- state reset, the classes' ticks (forked onto their streams and
+// joined), the copy of all proof states to pinned host memory -- is captured once into a
+// CUDA graph and replayed by every sc_batch_run. The reference has no batching (every proof
+// runs alone, with a blocking copy per interpolation point: cuda/src/field_sumcheck.cu:1012-1088).
 #include <algorithm>
 #include <vector>
 
@@ -15,57 +17,106 @@
 using namespace sc;
 using namespace sc_host;
 
+namespace {
+// Rounds with at least this many pairs derive g(1) from the claim (see capi.cu).
+constexpr uint64_t kBatchSkip1MinPairs = uint64_t{1} << 12;
+
+struct BatchClass {
+  int dclass = 2;
+  std::vector<int> proofs;
+  int threads = 256;
+  int grid = 1;
+  size_t smem = 0;
+  int max_rounds = 0;
+  std::vector<int> tick_round0, tick_item0, tick_items;  // offsets into the batch's arrays
+  int head0 = 0;                                         // this class's first queue counter
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> tick_events;                  // around every tick, inside the graph
+};
+}  // namespace
+
 struct sc_batch {
   sc_ctx* ctx = nullptr;
   const sc_field* field = nullptr;
-  int L = 0;
+  int L = 0, kind = 0;
   int count = 0;
   int mode = 0;
-  int threads = 256;
-  int grid = 0;
-  size_t smem = 0;
-  int max_rounds = 0;
+  int threads_req = 0, ppt = 2;
   std::vector<int> n, K, d;
   std::vector<StateOffsets> so;
   std::vector<size_t> state_base;  // word offset of each proof's state
   size_t state_words = 0;
-  std::vector<int> tick_round0, tick_rounds, tick_item0, tick_items;
+  std::vector<BatchClass> classes;
+  int total_heads = 0;
   DevBuf fold_pool, state, partials, rounds, items, heads, exprs;
   uint32_t* host_state = nullptr;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ready = nullptr, done = nullptr;
+  cudaEvent_t ready = nullptr, done = nullptr, fork = nullptr;
+  cudaEvent_t origin = nullptr;  // timing origin of a run (recorded inside the graph)
   cudaGraphExec_t exec = nullptr;
-  std::vector<float> tick_ms;  // per-tick device time of the last run
-  std::vector<cudaEvent_t> tick_events;  // recorded around every tick (inside the graph)
 };
 
 namespace {
 
+template <int L, int K, int D>
+struct BatchClassSetup {
+  static int run(sc_batch* B, BatchClass& C, int kmax) {
+    int threads = std::min(B->threads_req ? B->threads_req : kernel_threads(L), kernel_threads(L));
+    const int per_thread = round_smem_words_per_thread(kmax, L) * 4;
+    while (threads > 32 && static_cast<size_t>(threads) * per_thread > static_cast<size_t>(kMaxDynSmem)) threads -= 32;
+    C.threads = threads;
+    C.smem = static_cast<size_t>(threads) * per_thread;
+    SC_CUDA(cudaFuncSetAttribute(batch_round_kernel<L, K, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    int bps = 0;
+    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_round_kernel<L, K, D>, threads, C.smem));
+    if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "batch kernel does not fit on an SM (K=%d, L=%d)", kmax, L);
+    C.grid = bps * B->ctx->sm_count;
+    return SC_OK;
+  }
+};
+
+template <int L, int K, int D>
+struct BatchTick {
+  static int run(sc_batch* B, const BatchClass& C, int t, const BatchTickArgs& T) {
+    FieldParams<L, K> F;
+    for (int l = 0; l < L; ++l) F.p[l] = B->field->hf.p[l];
+    F.np = B->field->hf.np;
+    const unsigned grid = static_cast<unsigned>(std::min(C.grid, std::max(1, T.num_items)));
+    SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t], C.stream, cudaEventRecordExternal));
+    batch_round_kernel<L, K, D><<<grid, C.threads, C.smem, C.stream>>>(T, F);
+    SC_CUDA(cudaGetLastError());
+    SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t + 1], C.stream, cudaEventRecordExternal));
+    return SC_OK;
+  }
+};
+
 template <int L>
-int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const* tables, int ppt) {
+int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const* tables) {
   sc_ctx* ctx = B->ctx;
   const int count = B->count;
   int rc;
-  // expressions
   std::vector<ExprDev> ed(count);
-  int kmax = 1;
   for (int p = 0; p < count; ++p) {
     build_expr_dev<L>(*exprs[p], *B->field, ed[p]);
     B->K.push_back(exprs[p]->num_vars);
     B->d.push_back(exprs[p]->degree);
-    kmax = std::max(kmax, exprs[p]->num_vars);
   }
-  // launch shape
-  int threads = B->threads;
-  const int per_thread = round_smem_words_per_thread(kmax, L) * 4;
-  while (threads > 32 && static_cast<size_t>(threads) * per_thread > static_cast<size_t>(kMaxDynSmem)) threads -= 32;
-  B->threads = threads;
-  B->smem = static_cast<size_t>(threads) * per_thread;
-  SC_CUDA(cudaFuncSetAttribute(batch_round_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-  int bps = 0;
-  SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_round_kernel<L>, threads, B->smem));
-  if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "batch kernel does not fit on an SM (K=%d, L=%d)", kmax, L);
-  B->grid = bps * ctx->sm_count;
+  // degree classes
+  for (int dc : {2, 4, 7}) {
+    BatchClass C;
+    C.dclass = dc;
+    int kmax = 1;
+    for (int p = 0; p < count; ++p)
+      if (degree_class(B->d[p]) == dc) {
+        C.proofs.push_back(p);
+        kmax = std::max(kmax, B->K[p]);
+        C.max_rounds = std::max(C.max_rounds, B->n[p]);
+      }
+    if (C.proofs.empty()) continue;
+    if ((rc = dispatch<BatchClassSetup>(L, B->kind, dc, B, C, kmax))) return rc;
+    B->classes.push_back(std::move(C));
+  }
   // per-proof state and fold buffers (16-byte aligned carve-outs of two pools)
   std::vector<size_t> fold_a(count), fold_b(count);
   size_t fold_words = 0;
@@ -85,69 +136,74 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
   SC_CUDA(cudaMallocHost(&B->host_state, B->state_words * 4));
   uint32_t* st = static_cast<uint32_t*>(B->state.p);
   uint32_t* pool = static_cast<uint32_t*>(B->fold_pool.p);
-  // ticks: rounds and items
+  // every class's ticks: rounds and items, in one array each (class and tick offsets)
   std::vector<BatchRound> rounds;
   std::vector<BatchItem> items;
-  for (int t = 0; t < B->max_rounds; ++t) {
-    B->tick_round0.push_back(static_cast<int>(rounds.size()));
-    B->tick_item0.push_back(static_cast<int>(items.size()));
-    int tick_rounds = 0, tick_items = 0;
-    for (int p = 0; p < count; ++p) {
-      if (t >= B->n[p]) continue;
-      const uint64_t N = uint64_t{1} << B->n[p];
-      BatchRound R;
-      std::memset(&R, 0, sizeof(R));
-      RoundArgs& A = R.args;
-      A.round = t;
-      A.num_rounds = B->n[p];
-      A.mode = B->mode;
-      A.fc = B->field->dev;
-      A.pairs = N >> (t + 1);
-      if (t == 0) {
-        A.fold = 0;
-        A.src = tables[p];
-        A.src_len = N;
-      } else {
-        A.fold = 1;
-        A.src_len = N >> (t - 1);
-        A.src = t == 1 ? tables[p] : pool + ((t & 1) ? fold_b[p] : fold_a[p]);
-        A.dst = pool + ((t & 1) ? fold_a[p] : fold_b[p]);
+  for (BatchClass& C : B->classes) {
+    C.head0 = B->total_heads;
+    B->total_heads += C.max_rounds;
+    for (int t = 0; t < C.max_rounds; ++t) {
+      C.tick_round0.push_back(static_cast<int>(rounds.size()));
+      C.tick_item0.push_back(static_cast<int>(items.size()));
+      int tick_items = 0;
+      for (int p : C.proofs) {
+        if (t >= B->n[p]) continue;
+        const int n = B->n[p];
+        const uint64_t N = uint64_t{1} << n;
+        BatchRound R;
+        std::memset(&R, 0, sizeof(R));
+        RoundArgs& A = R.args;
+        A.round = t;
+        A.num_rounds = n;
+        A.mode = B->mode;
+        A.fc = B->field->dev;
+        A.pairs = N >> (t + 1);
+        A.skip1 = (t >= 1 && A.pairs >= kBatchSkip1MinPairs) ? 1 : 0;
+        A.want_claim = (t + 1 < n && (N >> (t + 2)) >= kBatchSkip1MinPairs) ? 1 : 0;
+        if (t == 0) {
+          A.fold = 0;
+          A.src = tables[p];
+          A.src_len = N;
+        } else {
+          A.fold = 1;
+          A.src_len = N >> (t - 1);
+          A.src = t == 1 ? tables[p] : pool + ((t & 1) ? fold_b[p] : fold_a[p]);
+          A.dst = pool + ((t & 1) ? fold_a[p] : fold_b[p]);
+        }
+        uint32_t* s = st + B->state_base[p];
+        const StateOffsets& o = B->so[p];
+        A.st.counter = s + o.counter;
+        A.st.status = s + o.status;
+        A.st.checksum = reinterpret_cast<uint64_t*>(s + o.checksum);
+        A.st.polys = s + o.polys;
+        A.st.chals = s + o.chals;
+        A.st.finals = s + o.finals;
+        A.st.claim0 = s + o.claim0;
+        A.st.claim = s + o.claim;
+        R.expr = p;
+        const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt;
+        const uint64_t nitems = (A.pairs + tile - 1) / tile;
+        R.first_item = static_cast<int>(items.size()) - C.tick_item0[t];  // tick-relative
+        R.num_items = static_cast<int>(nitems);
+        const int ridx = static_cast<int>(rounds.size()) - C.tick_round0[t];
+        for (uint64_t i = 0; i < nitems; ++i) {
+          BatchItem I;
+          I.round = ridx;
+          I.pad = 0;
+          I.start = i * tile;
+          I.count = std::min<uint64_t>(tile, A.pairs - i * tile);
+          items.push_back(I);
+        }
+        rounds.push_back(R);
+        tick_items += static_cast<int>(nitems);
       }
-      uint32_t* s = st + B->state_base[p];
-      const StateOffsets& o = B->so[p];
-      A.st.counter = s + o.counter;
-      A.st.status = s + o.status;
-      A.st.checksum = reinterpret_cast<uint64_t*>(s + o.checksum);
-      A.st.polys = s + o.polys;
-      A.st.chals = s + o.chals;
-      A.st.finals = s + o.finals;
-      A.st.claim0 = s + o.claim0;
-      R.expr = p;
-      const uint64_t tile = static_cast<uint64_t>(threads) * ppt;
-      const uint64_t nitems = (A.pairs + tile - 1) / tile;
-      R.first_item = static_cast<int>(items.size()) - B->tick_item0[t];  // tick-relative
-      R.num_items = static_cast<int>(nitems);
-      const int ridx = static_cast<int>(rounds.size()) - B->tick_round0[t];
-      for (uint64_t i = 0; i < nitems; ++i) {
-        BatchItem I;
-        I.round = ridx;
-        I.pad = 0;
-        I.start = i * tile;
-        I.count = std::min<uint64_t>(tile, A.pairs - i * tile);
-        items.push_back(I);
-      }
-      rounds.push_back(R);
-      ++tick_rounds;
-      tick_items += static_cast<int>(nitems);
+      C.tick_items.push_back(tick_items);
     }
-    B->tick_rounds.push_back(tick_rounds);
-    B->tick_items.push_back(tick_items);
   }
-  // partial index = global item index
   if ((rc = ensure(ctx, B->partials, items.size() * kMaxPoints * L * 4))) return rc;
   if ((rc = ensure(ctx, B->rounds, rounds.size() * sizeof(BatchRound)))) return rc;
   if ((rc = ensure(ctx, B->items, items.size() * sizeof(BatchItem)))) return rc;
-  if ((rc = ensure(ctx, B->heads, static_cast<size_t>(B->max_rounds) * 4))) return rc;
+  if ((rc = ensure(ctx, B->heads, static_cast<size_t>(std::max(1, B->total_heads)) * 4))) return rc;
   if ((rc = ensure(ctx, B->exprs, ed.size() * sizeof(ExprDev)))) return rc;
   SC_CUDA(cudaMemcpy(B->rounds.p, rounds.data(), rounds.size() * sizeof(BatchRound), cudaMemcpyHostToDevice));
   SC_CUDA(cudaMemcpy(B->items.p, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
@@ -156,39 +212,30 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
 }
 
 // The launch sequence of one run (captured once into the graph).
-template <int L>
 int batch_issue(sc_batch* B) {
-  FieldParams<L> F;
-  for (int l = 0; l < L; ++l) F.p[l] = B->field->hf.p[l];
-  F.np = B->field->hf.np;
   SC_CUDA(cudaMemsetAsync(B->state.p, 0, B->state_words * 4, B->stream));
-  SC_CUDA(cudaMemsetAsync(B->heads.p, 0, static_cast<size_t>(B->max_rounds) * 4, B->stream));
-  for (int t = 0; t < B->max_rounds; ++t) {
-    BatchTickArgs T;
-    T.rounds = static_cast<const BatchRound*>(B->rounds.p) + B->tick_round0[t];
-    T.items = static_cast<const BatchItem*>(B->items.p) + B->tick_item0[t];
-    T.num_items = B->tick_items[t];
-    T.pad = 0;
-    T.head = static_cast<uint32_t*>(B->heads.p) + t;
-    T.exprs = static_cast<const ExprDev*>(B->exprs.p);
-    T.partials = static_cast<uint32_t*>(B->partials.p) + static_cast<size_t>(B->tick_item0[t]) * kMaxPoints * L;
-    const unsigned grid = static_cast<unsigned>(std::min(B->grid, std::max(1, T.num_items)));
-    SC_CUDA(cudaEventRecordWithFlags(B->tick_events[2 * t], B->stream, cudaEventRecordExternal));
-    batch_round_kernel<L><<<grid, B->threads, B->smem, B->stream>>>(T, F);
-    SC_CUDA(cudaGetLastError());
-    SC_CUDA(cudaEventRecordWithFlags(B->tick_events[2 * t + 1], B->stream, cudaEventRecordExternal));
+  SC_CUDA(cudaMemsetAsync(B->heads.p, 0, static_cast<size_t>(std::max(1, B->total_heads)) * 4, B->stream));
+  SC_CUDA(cudaEventRecordWithFlags(B->origin, B->stream, cudaEventRecordExternal));
+  SC_CUDA(cudaEventRecord(B->fork, B->stream));
+  for (BatchClass& C : B->classes) {
+    SC_CUDA(cudaStreamWaitEvent(C.stream, B->fork, 0));
+    for (int t = 0; t < C.max_rounds; ++t) {
+      BatchTickArgs T;
+      T.rounds = static_cast<const BatchRound*>(B->rounds.p) + C.tick_round0[t];
+      T.items = static_cast<const BatchItem*>(B->items.p) + C.tick_item0[t];
+      T.num_items = C.tick_items[t];
+      T.pad = 0;
+      T.head = static_cast<uint32_t*>(B->heads.p) + C.head0 + t;
+      T.exprs = static_cast<const ExprDev*>(B->exprs.p);
+      T.partials = static_cast<uint32_t*>(B->partials.p) + static_cast<size_t>(C.tick_item0[t]) * kMaxPoints * B->L;
+      const int rc = dispatch<BatchTick>(B->L, B->kind, C.dclass, B, C, t, T);
+      if (rc) return rc;
+    }
+    SC_CUDA(cudaEventRecord(C.done, C.stream));
+    SC_CUDA(cudaStreamWaitEvent(B->stream, C.done, 0));
   }
   SC_CUDA(cudaMemcpyAsync(B->host_state, B->state.p, B->state_words * 4, cudaMemcpyDeviceToHost, B->stream));
   return SC_OK;
-}
-
-int batch_issue_any(sc_batch* B) {
-  switch (B->L) {
-    case 1: return batch_issue<1>(B);
-    case 2: return batch_issue<2>(B);
-    case 4: return batch_issue<4>(B);
-    default: return batch_issue<8>(B);
-  }
 }
 
 }  // namespace
@@ -217,31 +264,36 @@ int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr
   B->ctx = ctx;
   B->field = field;
   B->L = field->hf.L;
+  B->kind = field_kind(field->hf.p, B->L);
   B->count = count;
   B->mode = challenge_mode;
-  B->threads = threads ? threads : 256;
-  for (int p = 0; p < count; ++p) {
-    B->n.push_back(num_rounds[p]);
-    B->max_rounds = std::max(B->max_rounds, num_rounds[p]);
-  }
-  const int ppt = pairs_per_thread ? pairs_per_thread : 2;
+  B->threads_req = threads;
+  B->ppt = pairs_per_thread ? pairs_per_thread : 2;
+  for (int p = 0; p < count; ++p) B->n.push_back(num_rounds[p]);
   int rc;
   switch (B->L) {
-    case 1: rc = batch_setup<1>(B, exprs, tables_dev, ppt); break;
-    case 2: rc = batch_setup<2>(B, exprs, tables_dev, ppt); break;
-    case 4: rc = batch_setup<4>(B, exprs, tables_dev, ppt); break;
-    default: rc = batch_setup<8>(B, exprs, tables_dev, ppt); break;
+    case 1: rc = batch_setup<1>(B, exprs, tables_dev); break;
+    case 2: rc = batch_setup<2>(B, exprs, tables_dev); break;
+    case 4: rc = batch_setup<4>(B, exprs, tables_dev); break;
+    default: rc = batch_setup<8>(B, exprs, tables_dev); break;
   }
   cudaError_t e = cudaSuccess;
   if (!rc) e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
-  for (int i = 0; !rc && e == cudaSuccess && i < 2 * B->max_rounds; ++i) {
-    cudaEvent_t ev;
-    e = cudaEventCreate(&ev);
-    if (e == cudaSuccess) B->tick_events.push_back(ev);
-  }
   if (!rc && e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ready, cudaEventDisableTiming);
   if (!rc && e == cudaSuccess) e = cudaEventCreateWithFlags(&B->done, cudaEventDisableTiming);
-  if (!rc && e != cudaSuccess) rc = fail(SC_ERR_CUDA, "batch stream/events: %s", cudaGetErrorString(e));
+  if (!rc && e == cudaSuccess) e = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
+  if (!rc && e == cudaSuccess) e = cudaEventCreate(&B->origin);
+  for (size_t c = 0; !rc && e == cudaSuccess && c < B->classes.size(); ++c) {
+    BatchClass& C = B->classes[c];
+    e = cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&C.done, cudaEventDisableTiming);
+    for (int i = 0; e == cudaSuccess && i < 2 * C.max_rounds; ++i) {
+      cudaEvent_t ev;
+      e = cudaEventCreate(&ev);
+      if (e == cudaSuccess) C.tick_events.push_back(ev);
+    }
+  }
+  if (!rc && e != cudaSuccess) rc = fail(SC_ERR_CUDA, "batch streams/events: %s", cudaGetErrorString(e));
   if (rc) {
     sc_batch_destroy(B);
     return rc;
@@ -256,11 +308,10 @@ int sc_batch_run(sc_batch* B) {
   // the batch starts after the work already queued on the caller's stream
   SC_CUDA(cudaEventRecord(B->ready, B->ctx->stream));
   SC_CUDA(cudaStreamWaitEvent(B->stream, B->ready, 0));
-  int rc;
   if (!B->exec) {
     cudaGraph_t g = nullptr;
     SC_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
-    rc = batch_issue_any(B);
+    const int rc = batch_issue(B);
     cudaError_t e = cudaStreamEndCapture(B->stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -280,19 +331,46 @@ int sc_batch_run(sc_batch* B) {
 int sc_batch_wait(sc_batch* B) {
   if (!B) return fail(SC_ERR_INVALID, "NULL batch");
   SC_CUDA(cudaEventSynchronize(B->done));
-  B->tick_ms.assign(B->max_rounds, 0.f);
-  for (int t = 0; t < B->max_rounds; ++t)
-    SC_CUDA(cudaEventElapsedTime(&B->tick_ms[t], B->tick_events[2 * t], B->tick_events[2 * t + 1]));
   for (int p = 0; p < B->count; ++p)
     if (B->host_state[B->state_base[p] + B->so[p].status])
       return fail(SC_ERR_DEVICE, "proof %d: device status %u", p, B->host_state[B->state_base[p] + B->so[p].status]);
   return SC_OK;
 }
 
-int sc_batch_tick_times(sc_batch* B, float* out_ms, int capacity, int* count) {
+int sc_batch_tick_times(sc_batch* B, float* out_start_ms, float* out_end_ms, int capacity, int* count) {
   if (!B || !count) return fail(SC_ERR_INVALID, "NULL argument");
-  *count = static_cast<int>(B->tick_ms.size());
-  for (int i = 0; out_ms && i < *count && i < capacity; ++i) out_ms[i] = B->tick_ms[i];
+  int k = 0;
+  for (const BatchClass& C : B->classes) k += C.max_rounds;
+  *count = k;
+  int i = 0;
+  for (const BatchClass& C : B->classes)
+    for (int t = 0; t < C.max_rounds; ++t, ++i) {
+      if (i >= capacity) continue;
+      float a = 0.f, b = 0.f;
+      SC_CUDA(cudaEventElapsedTime(&a, B->origin, C.tick_events[2 * t]));
+      SC_CUDA(cudaEventElapsedTime(&b, B->origin, C.tick_events[2 * t + 1]));
+      if (out_start_ms) out_start_ms[i] = a;
+      if (out_end_ms) out_end_ms[i] = b;
+    }
+  return SC_OK;
+}
+
+int sc_batch_classes(sc_batch* B, int32_t* out_degree_class, int32_t* out_ticks, int capacity, int* count) {
+  if (!B || !count) return fail(SC_ERR_INVALID, "NULL argument");
+  *count = static_cast<int>(B->classes.size());
+  for (int c = 0; c < *count && c < capacity; ++c) {
+    if (out_degree_class) out_degree_class[c] = B->classes[c].dclass;
+    if (out_ticks) out_ticks[c] = B->classes[c].max_rounds;
+  }
+  return SC_OK;
+}
+
+int sc_batch_class_proofs(sc_batch* B, int cls, int32_t* out_indices, int capacity, int* count) {
+  if (!B || !count) return fail(SC_ERR_INVALID, "NULL argument");
+  if (cls < 0 || cls >= static_cast<int>(B->classes.size())) return fail(SC_ERR_INVALID, "class %d", cls);
+  const auto& v = B->classes[cls].proofs;
+  *count = static_cast<int>(v.size());
+  for (int i = 0; out_indices && i < *count && i < capacity; ++i) out_indices[i] = v[i];
   return SC_OK;
 }
 
@@ -322,9 +400,15 @@ int sc_batch_destroy(sc_batch* B) {
   for (DevBuf* b : {&B->fold_pool, &B->state, &B->partials, &B->rounds, &B->items, &B->heads, &B->exprs})
     if (b->p) cudaFree(b->p);
   if (B->host_state) cudaFreeHost(B->host_state);
-  for (cudaEvent_t e : B->tick_events) cudaEventDestroy(e);
+  for (BatchClass& C : B->classes) {
+    for (cudaEvent_t e : C.tick_events) cudaEventDestroy(e);
+    if (C.done) cudaEventDestroy(C.done);
+    if (C.stream) cudaStreamDestroy(C.stream);
+  }
   if (B->ready) cudaEventDestroy(B->ready);
   if (B->done) cudaEventDestroy(B->done);
+  if (B->fork) cudaEventDestroy(B->fork);
+  if (B->origin) cudaEventDestroy(B->origin);
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
   return SC_OK;

@@ -12,103 +12,115 @@ using namespace sc_host;
 
 namespace {
 
-template <int L>
-int prove_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables,
-               int mode, const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch,
-               uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum) {
-  const int K = ex->num_vars, d = ex->degree;
-  const uint64_t N = uint64_t{1} << n;
-  // scratch
-  const size_t fold_a_words = n >= 2 ? static_cast<size_t>(K) * L * (N / 2) : 0;
-  const size_t fold_b_words = n >= 3 ? static_cast<size_t>(K) * L * (N / 4) : 0;
-  int rc;
-  if ((rc = ensure(ctx, ctx->fold_a, fold_a_words * 4))) return rc;
-  if ((rc = ensure(ctx, ctx->fold_b, fold_b_words * 4))) return rc;
-  const StateOffsets so = state_offsets(n, K, L);
-  if ((rc = ensure(ctx, ctx->state, so.total_words * 4))) return rc;
+// Rounds with at least this many pairs derive g(1) from the claim instead of evaluating
+// point 1; the previous round then interpolates g_{j-1}(r_{j-1}) in its finalisation, a
+// latency only worth paying when the round is large.
+constexpr uint64_t kSkip1MinPairs = uint64_t{1} << 12;
 
-  int threads = kBlock;
-  const int per_thread = round_smem_words_per_thread(K, L) * 4;
-  while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
-  const size_t smem = static_cast<size_t>(threads) * per_thread;
-  int blocks_per_sm = 0;
-  SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, round_kernel<L>, threads, smem));
-  if (blocks_per_sm < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K, L);
-  const uint64_t grid_max = static_cast<uint64_t>(blocks_per_sm) * ctx->sm_count;
-  if ((rc = ensure(ctx, ctx->partials, grid_max * kMaxPoints * L * 4))) return rc;
+inline bool round_skip1(int n, int j) { return j >= 1 && (uint64_t{1} << (n - j - 1)) >= kSkip1MinPairs; }
 
-  ExprDev E;
-  build_expr_dev<L>(*ex, *f, E);
-  FieldParams<L> F;
-  for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
-  F.np = f->hf.np;
+template <int L, int K, int DMAX>
+struct ProveRun {
+  static int run(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables, int mode,
+                 const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch, uint32_t* out_finals,
+                 uint32_t* out_claim0, uint64_t* out_checksum) {
+    const int K_ = ex->num_vars, d = ex->degree;
+    const uint64_t N = uint64_t{1} << n;
+    // scratch
+    const size_t fold_a_words = n >= 2 ? static_cast<size_t>(K_) * L * (N / 2) : 0;
+    const size_t fold_b_words = n >= 3 ? static_cast<size_t>(K_) * L * (N / 4) : 0;
+    int rc;
+    if ((rc = ensure(ctx, ctx->fold_a, fold_a_words * 4))) return rc;
+    if ((rc = ensure(ctx, ctx->fold_b, fold_b_words * 4))) return rc;
+    const StateOffsets so = state_offsets(n, K_, L);
+    if ((rc = ensure(ctx, ctx->state, so.total_words * 4))) return rc;
 
-  uint32_t* st = static_cast<uint32_t*>(ctx->state.p);
-  SC_CUDA(cudaMemsetAsync(st, 0, so.total_words * 4, ctx->stream));
-  if (mode == SC_CHALLENGE_EXPLICIT)
-    SC_CUDA(cudaMemcpyAsync(st + so.chals, explicit_ch, static_cast<size_t>(n) * L * 4,
-                            cudaMemcpyHostToDevice, ctx->stream));
+    int threads = kernel_threads(L);
+    const int per_thread = round_smem_words_per_thread(K_, L) * 4;
+    while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
+    const size_t smem = static_cast<size_t>(threads) * per_thread;
+    int blocks_per_sm = 0;
+    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, round_kernel<L, K, DMAX>, threads, smem));
+    if (blocks_per_sm < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K_, L);
+    const uint64_t grid_max = static_cast<uint64_t>(blocks_per_sm) * ctx->sm_count;
+    if ((rc = ensure(ctx, ctx->partials, grid_max * kMaxPoints * L * 4))) return rc;
 
-  RoundArgs A;
-  A.num_rounds = n;
-  A.mode = mode;
-  A.partials = static_cast<uint32_t*>(ctx->partials.p);
-  A.fc = f->dev;
-  A.st.counter = st + so.counter;
-  A.st.status = st + so.status;
-  A.st.checksum = reinterpret_cast<uint64_t*>(st + so.checksum);
-  A.st.polys = st + so.polys;
-  A.st.chals = st + so.chals;
-  A.st.finals = st + so.finals;
-  A.st.claim0 = st + so.claim0;
+    ExprDev E;
+    build_expr_dev<L>(*ex, *f, E);
+    FieldParams<L, K> F;
+    for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
+    F.np = f->hf.np;
 
-  const uint32_t* prev = tables;  // T_{j-1} (or T_0)
-  for (int j = 0; j < n; ++j) {
-    A.round = j;
-    A.pairs = N >> (j + 1);
-    if (j == 0) {
-      A.fold = 0;
-      A.src = tables;
-      A.dst = nullptr;
-      A.src_len = N;
-    } else {
-      A.fold = 1;
-      A.src = prev;
-      A.src_len = N >> (j - 1);
-      A.dst = static_cast<uint32_t*>((j & 1) ? ctx->fold_a.p : ctx->fold_b.p);
-      prev = A.dst;
+    uint32_t* st = static_cast<uint32_t*>(ctx->state.p);
+    SC_CUDA(cudaMemsetAsync(st, 0, so.total_words * 4, ctx->stream));
+    if (mode == SC_CHALLENGE_EXPLICIT)
+      SC_CUDA(cudaMemcpyAsync(st + so.chals, explicit_ch, static_cast<size_t>(n) * L * 4, cudaMemcpyHostToDevice,
+                              ctx->stream));
+
+    RoundArgs A;
+    A.num_rounds = n;
+    A.mode = mode;
+    A.partials = static_cast<uint32_t*>(ctx->partials.p);
+    A.fc = f->dev;
+    A.st.counter = st + so.counter;
+    A.st.status = st + so.status;
+    A.st.checksum = reinterpret_cast<uint64_t*>(st + so.checksum);
+    A.st.polys = st + so.polys;
+    A.st.chals = st + so.chals;
+    A.st.finals = st + so.finals;
+    A.st.claim0 = st + so.claim0;
+    A.st.claim = st + so.claim;
+
+    const uint32_t* prev = tables;  // T_{j-1} (or T_0)
+    for (int j = 0; j < n; ++j) {
+      A.round = j;
+      A.pairs = N >> (j + 1);
+      A.skip1 = round_skip1(n, j) ? 1 : 0;
+      A.want_claim = (j + 1 < n && round_skip1(n, j + 1)) ? 1 : 0;
+      if (j == 0) {
+        A.fold = 0;
+        A.src = tables;
+        A.dst = nullptr;
+        A.src_len = N;
+      } else {
+        A.fold = 1;
+        A.src = prev;
+        A.src_len = N >> (j - 1);
+        A.dst = static_cast<uint32_t*>((j & 1) ? ctx->fold_a.p : ctx->fold_b.p);
+        prev = A.dst;
+      }
+      const uint64_t want = (A.pairs + threads - 1) / threads;
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
+      cudaEvent_t ev;
+      if ((rc = timing_begin(ctx, &ev))) return rc;
+      round_kernel<L, K, DMAX><<<grid, threads, smem, ctx->stream>>>(A, E, F);
+      SC_CUDA(cudaGetLastError());
+      if ((rc = timing_end(ctx))) return rc;
     }
-    const uint64_t want = (A.pairs + threads - 1) / threads;
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
-    cudaEvent_t ev;
-    if ((rc = timing_begin(ctx, &ev))) return rc;
-    round_kernel<L><<<grid, threads, smem, ctx->stream>>>(A, E, F);
-    SC_CUDA(cudaGetLastError());
-    if ((rc = timing_end(ctx))) return rc;
+    // results
+    if (ctx->host_state_bytes < so.total_words * 4) {
+      if (ctx->host_state) cudaFreeHost(ctx->host_state);
+      ctx->host_state = nullptr;
+      ctx->host_state_bytes = 0;
+      SC_CUDA(cudaMallocHost(&ctx->host_state, so.total_words * 4));
+      ctx->host_state_bytes = so.total_words * 4;
+    }
+    SC_CUDA(cudaMemcpyAsync(ctx->host_state, st, so.total_words * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SC_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((rc = timing_collect(ctx))) return rc;
+    const uint32_t* hs = ctx->host_state;
+    if (hs[so.status]) return fail(SC_ERR_DEVICE, "device status %u", hs[so.status]);
+    if (out_polys)
+      for (int j = 0; j < n; ++j)
+        std::memcpy(out_polys + static_cast<size_t>(j) * (d + 1) * L, hs + so.polys + static_cast<size_t>(j) * kMaxPoints * L,
+                    static_cast<size_t>(d + 1) * L * 4);
+    if (out_ch) std::memcpy(out_ch, hs + so.chals, static_cast<size_t>(n) * L * 4);
+    if (out_finals) std::memcpy(out_finals, hs + so.finals, static_cast<size_t>(1 + K_) * L * 4);
+    if (out_claim0) std::memcpy(out_claim0, hs + so.claim0, L * 4);
+    if (out_checksum) std::memcpy(out_checksum, hs + so.checksum, 8);
+    return SC_OK;
   }
-  // results
-  if (ctx->host_state_bytes < so.total_words * 4) {
-    if (ctx->host_state) cudaFreeHost(ctx->host_state);
-    ctx->host_state = nullptr;
-    ctx->host_state_bytes = 0;
-    SC_CUDA(cudaMallocHost(&ctx->host_state, so.total_words * 4));
-    ctx->host_state_bytes = so.total_words * 4;
-  }
-  SC_CUDA(cudaMemcpyAsync(ctx->host_state, st, so.total_words * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  SC_CUDA(cudaStreamSynchronize(ctx->stream));
-  if ((rc = timing_collect(ctx))) return rc;
-  const uint32_t* hs = ctx->host_state;
-  if (hs[so.status]) return fail(SC_ERR_DEVICE, "device status %u", hs[so.status]);
-  if (out_polys)
-    for (int j = 0; j < n; ++j)
-      std::memcpy(out_polys + static_cast<size_t>(j) * (d + 1) * L, hs + so.polys + static_cast<size_t>(j) * kMaxPoints * L,
-                  static_cast<size_t>(d + 1) * L * 4);
-  if (out_ch) std::memcpy(out_ch, hs + so.chals, static_cast<size_t>(n) * L * 4);
-  if (out_finals) std::memcpy(out_finals, hs + so.finals, static_cast<size_t>(1 + K) * L * 4);
-  if (out_claim0) std::memcpy(out_claim0, hs + so.claim0, L * 4);
-  if (out_checksum) std::memcpy(out_checksum, hs + so.checksum, 8);
-  return SC_OK;
-}
+};
 
 template <int L>
 int generate_impl(sc_ctx* ctx, const sc_field* f, int num_tables, int n, const int32_t* kinds,
@@ -192,8 +204,7 @@ int sc_ctx_create(int device, void* stream, sc_ctx** out) {
     return fail(SC_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
   }
   int rc;
-  if ((rc = set_kernel_attrs<1>()) || (rc = set_kernel_attrs<2>()) || (rc = set_kernel_attrs<4>()) ||
-      (rc = set_kernel_attrs<8>())) {
+  if ((rc = for_each_instance<SetRoundAttrs>())) {
     delete c;
     return rc;
   }
@@ -472,12 +483,9 @@ int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_ro
   if (reinterpret_cast<uintptr_t>(tables_dev) % 16) return fail(SC_ERR_INVALID, "tables_dev must be 16-byte aligned");
   if (field->device != ctx->device) return fail(SC_ERR_INVALID, "field was set up on device %d, context is on %d", field->device, ctx->device);
   SC_CUDA(cudaSetDevice(ctx->device));
-  switch (field->hf.L) {
-    case 1: return prove_impl<1>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    case 2: return prove_impl<2>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    case 4: return prove_impl<4>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    default: return prove_impl<8>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-  }
+  return dispatch<ProveRun>(field->hf.L, field_kind(field->hf.p, field->hf.L), degree_class(expr->degree), ctx, field,
+                            expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys,
+                            out_challenges, out_finals, out_claim0, out_checksum);
 }
 
 }  // extern "C"

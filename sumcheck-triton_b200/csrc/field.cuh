@@ -5,7 +5,17 @@
 // unique, so they are what the transcript hashes and the checksum sums, exactly as in the
 // reference (cuda/src/field_sumcheck.cu:1046-1049, :857-907).
 //
-// The carry chains themselves are inline PTX in field_ptx.cuh (generated).
+// Which Montgomery product runs is chosen per limb count by measurement on B200 (a probe of
+// chained products per thread, 148 x 8 blocks; G products/s):
+//
+//   L = 1  inline-PTX mad.lo.cc / madc.hi.cc chain (field_ptx.cuh)     2.30  (C++ form 1.68)
+//   L = 2  Goldilocks modulus: the special reduction below              0.81
+//          any other modulus: CIOS with 64-bit intermediates (C++)     0.56  (PTX chains 0.51)
+//   L = 4  CIOS with 64-bit intermediates                               0.167 (PTX chains 0.157)
+//   L = 8  CIOS with 64-bit intermediates                               0.0466 (PTX chains 0.0417)
+//
+// All forms compute the same function: a b R^-1 mod p, fully reduced, for a, b < p. Modular
+// add and subtract are inline-PTX add.cc/addc and sub.cc/subc chains for every L.
 #pragma once
 #include <cstdint>
 
@@ -16,14 +26,16 @@ namespace sc {
 constexpr int kMaxLimbs = 8;
 constexpr int kMaxPoints = 8;  // t = 0..7, degree <= 7
 
+enum FieldKind : int { kFieldGeneric = 0, kFieldGoldilocks = 1 };
+
 template <int L>
 struct Fe {
   uint32_t w[L];
 };
 
 // The two constants every product needs. Passed by value as a kernel parameter, so it
-// lives in the constant bank and the multiply-adds read it from there.
-template <int L>
+// lives in the constant bank. KIND selects a special reduction for a known modulus.
+template <int L, int KIND = kFieldGeneric>
 struct FieldParams {
   uint32_t p[L];
   uint32_t np;  // -p^-1 mod 2^32
@@ -37,24 +49,95 @@ __device__ __forceinline__ Fe<L> fe_zero() {
   return z;
 }
 
-template <int L>
-__device__ __forceinline__ Fe<L> fe_add(const Fe<L>& a, const Fe<L>& b, const FieldParams<L>& F) {
+template <int L, int K>
+__device__ __forceinline__ Fe<L> fe_add(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
   ptx_add_mod<L>(r.w, a.w, b.w, F.p);
   return r;
 }
 
-template <int L>
-__device__ __forceinline__ Fe<L> fe_sub(const Fe<L>& a, const Fe<L>& b, const FieldParams<L>& F) {
+template <int L, int K>
+__device__ __forceinline__ Fe<L> fe_sub(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
   ptx_sub_mod<L>(r.w, a.w, b.w, F.p);
   return r;
 }
 
+// CIOS (Koc-Acar-Kaliski 1996) with 64-bit intermediates and a fully carried L+2-word
+// accumulator; the compiler chooses the multiply-add instructions.
 template <int L>
-__device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const FieldParams<L>& F) {
+__device__ __forceinline__ void cios_mul(uint32_t (&r)[L], const uint32_t (&a)[L], const uint32_t (&b)[L],
+                                         const uint32_t (&p)[L], uint32_t np) {
+  uint32_t t[L + 2];
+#pragma unroll
+  for (int i = 0; i < L + 2; ++i) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+      const uint64_t uv = static_cast<uint64_t>(a[j]) * b[i] + t[j] + c;
+      t[j] = static_cast<uint32_t>(uv);
+      c = uv >> 32;
+    }
+    uint64_t s = static_cast<uint64_t>(t[L]) + c;
+    t[L] = static_cast<uint32_t>(s);
+    t[L + 1] = static_cast<uint32_t>(s >> 32);
+    const uint32_t m = t[0] * np;
+    c = (static_cast<uint64_t>(m) * p[0] + t[0]) >> 32;
+#pragma unroll
+    for (int j = 1; j < L; ++j) {
+      const uint64_t uv = static_cast<uint64_t>(m) * p[j] + t[j] + c;
+      t[j - 1] = static_cast<uint32_t>(uv);
+      c = uv >> 32;
+    }
+    s = static_cast<uint64_t>(t[L]) + c;
+    t[L - 1] = static_cast<uint32_t>(s);
+    t[L] = t[L + 1] + static_cast<uint32_t>(s >> 32);
+    t[L + 1] = 0;
+  }
+  uint32_t d[L];
+  uint64_t br = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    const uint64_t x = static_cast<uint64_t>(t[i]) - p[i] - br;
+    d[i] = static_cast<uint32_t>(x);
+    br = (x >> 63) & 1;
+  }
+  const bool below = (t[L] == 0) && br;  // t < p: keep t
+#pragma unroll
+  for (int i = 0; i < L; ++i) r[i] = below ? t[i] : d[i];
+}
+
+// Montgomery product for p = 2^64 - 2^32 + 1 and R = 2^64 (x, y < p):
+// with x y = h 2^64 + l, -p^-1 = -(1 + 2^32) mod 2^64, so a = l (1 + 2^32) mod 2^64 (carry
+// e out of the 32-bit halves) satisfies x y - a p = 0 mod 2^64, and
+// (x y - a p) / 2^64 = h - b with b = a - (a >> 32) - e, 0 <= b < p; one conditional
+// addition of p makes h - b fully reduced. (Derivation in the comment of gold_mul's test.)
+__device__ __forceinline__ void gold_mul(uint32_t (&r)[2], const uint32_t (&x32)[2], const uint32_t (&y32)[2]) {
+  const uint64_t x = (static_cast<uint64_t>(x32[1]) << 32) | x32[0];
+  const uint64_t y = (static_cast<uint64_t>(y32[1]) << 32) | y32[0];
+  const uint64_t l = x * y;
+  const uint64_t h = __umul64hi(x, y);
+  const uint64_t a = l + (l << 32);
+  const uint64_t e = a < l ? 1u : 0u;
+  const uint64_t b = a - (a >> 32) - e;
+  uint64_t res = h - b;
+  if (h < b) res += 0xFFFFFFFF00000001ull;
+  r[0] = static_cast<uint32_t>(res);
+  r[1] = static_cast<uint32_t>(res >> 32);
+}
+
+template <int L, int K>
+__device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  ptx_mont_mul<L>(r.w, a.w, b.w, F.p, F.np);
+  if constexpr (K == kFieldGoldilocks && L == 2) {
+    gold_mul(r.w, a.w, b.w);
+  } else if constexpr (L == 1) {
+    ptx_mont_mul<1>(r.w, a.w, b.w, F.p, F.np);
+  } else {
+    cios_mul<L>(r.w, a.w, b.w, F.p, F.np);
+  }
   return r;
 }
 
@@ -66,12 +149,11 @@ __device__ __forceinline__ bool fe_is_zero(const Fe<L>& a) {
   return o == 0;
 }
 
-// Multiply by a small signed integer c by double-and-add (|c| < 2^31). The result equals
-// the Montgomery product with the Montgomery image of c; an addition chain is cheaper
-// than a product for the small coefficients constraint expressions carry.
-template <int L>
-__device__ __forceinline__ Fe<L> fe_mul_small(const Fe<L>& a, int32_t c, const FieldParams<L>& F) {
-  uint32_t m = c < 0 ? static_cast<uint32_t>(-static_cast<int64_t>(c)) : static_cast<uint32_t>(c);
+// Multiply by a small non-negative integer c by double-and-add. The result equals the
+// Montgomery product with c's Montgomery image; an addition chain is cheaper than a product
+// for the small coefficients constraint expressions carry.
+template <int L, int K>
+__device__ __forceinline__ Fe<L> fe_mul_small(const Fe<L>& a, uint32_t m, const FieldParams<L, K>& F) {
   Fe<L> acc = fe_zero<L>();
   Fe<L> base = a;
   bool first = true;
@@ -83,7 +165,6 @@ __device__ __forceinline__ Fe<L> fe_mul_small(const Fe<L>& a, int32_t c, const F
     m >>= 1;
     if (m) base = fe_add(base, base, F);
   }
-  if (c < 0) acc = fe_sub(fe_zero<L>(), acc, F);
   return acc;
 }
 

@@ -4,19 +4,22 @@ Run from the repository root (the build runs it when the header is missing or ol
 
     python sumcheck-triton_b200/csrc/gen_field_ptx.py
 
-Why a generator: every carry chain (``add.cc``/``addc``, ``mad.lo.cc``/``madc.hi.cc``) must sit
-inside ONE ``asm`` statement, because the carry flag is not preserved across statements
-(the compiler may schedule its own ``.cc`` instructions in between). A chain is as long as the
-limb count, so each limb count L in {1, 2, 4, 8} gets its own unrolled statements. Every
-chain emitted here ends in an instruction without ``.cc``, so no carry is live between
-statements.
+Each operation (Montgomery product, modular add, modular subtract) for a limb count L in
+{1, 2, 4, 8} is ONE asm statement, generated here as straight-line PTX:
+
+* the carry flag is only meaningful inside one statement (the compiler may place its own
+  ``.cc`` instructions between statements), so every chain must be inside one;
+* every intermediate lives in a PTX register declared inside the statement, and every
+  result operand is early-clobber (``=&r``), so no operand can share a register with a
+  value the statement still reads -- the compiler may otherwise merge operands that hold
+  equal values (e.g. ``m = t0 * nprime`` when nprime is 1).
 
 Montgomery product (CIOS, Koc-Acar-Kaliski 1996, "Analyzing and comparing Montgomery
 multiplication algorithms"), per outer iteration i:
 
     t += a * b[i]                  two chains: low halves into t[0..L], high halves into t[1..L]
     m  = t[0] * nprime mod 2^32
-    t  = (t + m * p) / 2^32        two chains, then a one-word shift
+    t  = (t + m * p) / 2^32        two chains; the one-word shift is a renaming of registers
 
 The accumulator between iterations is L+1 words; the a*b[i] chains therefore drop a carry out
 of word L, which is exact whenever (2p-1) + (p-1)(2^32-1) < 2^(32(L+1)) -- the bound the host
@@ -32,239 +35,163 @@ from pathlib import Path
 OUT = Path(__file__).resolve().parent / "field_ptx.cuh"
 
 
-def _asm(lines, outs, ins):
-    """One asm statement: lines use {o0..}/{i0..} placeholders for operands."""
-    nout = len(outs)
-    body = []
-    for ln in lines:
-        for k in range(len(outs)):
-            ln = ln.replace(f"{{o{k}}}", f"%{k}")
-        for k in range(len(ins)):
-            ln = ln.replace(f"{{i{k}}}", f"%{nout + k}")
-        body.append(ln)
-    text = "\\n\\t\"\n        \"".join(body)
-    o = ", ".join(outs)
-    i = ", ".join(ins)
-    return f'    asm(\n        "{text}"\n        : {o}\n        : {i});\n'
+class Asm:
+    """Builds one asm statement: PTX lines over named operands and local registers."""
+
+    def __init__(self, outs, ins):
+        self.outs = outs  # [(name, c_expr)]
+        self.ins = ins  # [(name, c_expr)]
+        self.lines = []
+        self.locals_u32 = []
+        self.locals_pred = []
+
+    def ref(self, name):
+        for k, (n, _e) in enumerate(self.outs):
+            if n == name:
+                return f"%{k}"
+        for k, (n, _e) in enumerate(self.ins):
+            if n == name:
+                return f"%{len(self.outs) + k}"
+        return name  # a local register
+
+    def op(self, text, *names):
+        self.lines.append(text.format(*[self.ref(n) for n in names]))
+
+    def render(self, indent="    "):
+        body = ["{"]
+        if self.locals_u32:
+            body.append(".reg .u32 " + ", ".join(self.locals_u32) + ";")
+        if self.locals_pred:
+            body.append(".reg .pred " + ", ".join(self.locals_pred) + ";")
+        body += self.lines + ["}"]
+        text = ("\\n\\t\"\n" + indent + "    \"").join(body)
+        outs = ", ".join(f'"=&r"({e})' for _n, e in self.outs)
+        ins = ", ".join(f'"r"({e})' for _n, e in self.ins)
+        return f'{indent}asm("{text}"\n{indent}    : {outs}\n{indent}    : {ins});\n'
 
 
 def gen_mont_mul(L: int) -> str:
-    """CIOS with an (L+1)-word accumulator t[0..L] and a transient t[L+1]."""
-    s = []
-    s.append(
+    head = (
         f"template <> __device__ __forceinline__ void ptx_mont_mul<{L}>(uint32_t (&r)[{L}], "
-        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}], "
-        f"uint32_t np) {{\n"
+        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}], uint32_t np) {{\n"
     )
+    outs = [(f"r{j}", f"r[{j}]") for j in range(L)]
+    ins = [(f"a{j}", f"a[{j}]") for j in range(L)] + [(f"b{j}", f"b[{j}]") for j in range(L)]
+    ins += [(f"p{j}", f"p[{j}]") for j in range(L)] + [("np", "np")]
+    A = Asm(outs, ins)
     if L == 1:
-        s.append("    uint32_t hi, c;\n")
-        s.append(
-            _asm(
-                [
-                    "{",
-                    ".reg .u32 lo, m;",
-                    "mul.lo.u32 lo, {i0}, {i1};",
-                    "mul.hi.u32 {o0}, {i0}, {i1};",
-                    "mul.lo.u32 m, lo, {i3};",
-                    "mad.lo.cc.u32 lo, m, {i2}, lo;",
-                    "madc.hi.cc.u32 {o0}, m, {i2}, {o0};",
-                    "addc.u32 {o1}, 0, 0;",
-                    "}",
-                ],
-                ['"=&r"(hi)', '"=&r"(c)'],
-                ['"r"(a[0])', '"r"(b[0])', '"r"(p[0])', '"r"(np)'],
-            )
-        )
-        s.append("    uint32_t d, bw;\n")
-        s.append(
-            _asm(
-                ["sub.cc.u32 {o0}, {i0}, {i2};", "subc.u32 {o1}, {i1}, 0;"],
-                ['"=&r"(d)', '"=&r"(bw)'],
-                ['"r"(hi)', '"r"(c)', '"r"(p[0])'],
-            )
-        )
-        s.append("    r[0] = bw ? hi : d;\n}\n\n")
-        return "".join(s)
-
-    s.append(f"    uint32_t t[{L + 2}];\n")
-    # iteration 0: t = a * b[0] (no accumulate)
-    lo = [f"mul.lo.u32 {{o{j}}}, {{i{j}}}, {{i{L}}};" for j in range(L)]
-    lo.append(f"mov.u32 {{o{L}}}, 0;")
-    s.append(
-        _asm(
-            lo,
-            [f'"=&r"(t[{j}])' for j in range(L + 1)],
-            [f'"r"(a[{j}])' for j in range(L)] + ['"r"(b[0])'],
-        )
-    )
-    hi = []
+        A.locals_u32 = ["lo", "hi", "m", "c", "d", "bw"]
+        A.locals_pred = ["keep"]
+        A.op("mul.lo.u32 lo, {}, {};", "a0", "b0")
+        A.op("mul.hi.u32 hi, {}, {};", "a0", "b0")
+        A.op("mul.lo.u32 m, lo, {};", "np")
+        A.op("mad.lo.cc.u32 lo, m, {}, lo;", "p0")
+        A.op("madc.hi.cc.u32 hi, m, {}, hi;", "p0")
+        A.op("addc.u32 c, 0, 0;")
+        A.op("sub.cc.u32 d, hi, {};", "p0")
+        A.op("subc.u32 bw, c, 0;")
+        A.op("setp.ne.u32 keep, bw, 0;")
+        A.op("selp.b32 {}, hi, d, keep;", "r0")
+        return head + A.render() + "}\n\n"
+    # physical accumulator registers x0..x{L+1}; logical t[k] is phys[k]
+    A.locals_u32 = [f"x{k}" for k in range(L + 2)] + ["m"] + [f"d{k}" for k in range(L)] + ["bw"]
+    A.locals_pred = ["keep"]
+    phys = [f"x{k}" for k in range(L + 2)]
+    # iteration 0: t = a * b0
+    for j in range(L):
+        A.op(f"mul.lo.u32 {phys[j]}, {{}}, {{}};", f"a{j}", "b0")
+    A.op(f"mov.u32 {phys[L]}, 0;")
     for j in range(L):
         op = "mad.hi.cc.u32" if j == 0 else ("madc.hi.u32" if j == L - 1 else "madc.hi.cc.u32")
-        hi.append(f"{op} {{o{j + 1}}}, {{i{j}}}, {{i{L}}}, {{o{j + 1}}};")
-    s.append(
-        _asm(
-            hi,
-            [f'"+r"(t[{j}])' for j in range(L + 1)],
-            [f'"r"(a[{j}])' for j in range(L)] + ['"r"(b[0])'],
-        )
-    )
-    s.append("#pragma unroll\n")
-    s.append(f"    for (int i = 0; i < {L}; ++i) {{\n")
-    s.append("      if (i > 0) {\n")
-    # t += a * b[i]: low halves
-    lo = []
-    for j in range(L):
-        op = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
-        lo.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L}}}, {{o{j}}};")
-    lo.append(f"addc.u32 {{o{L}}}, {{o{L}}}, 0;")
-    s.append(
-        _asm(
-            lo,
-            [f'"+r"(t[{j}])' for j in range(L + 1)],
-            [f'"r"(a[{j}])' for j in range(L)] + ['"r"(b[i])'],
-        ).replace("\n    ", "\n      ").replace("    asm", "      asm", 1)
-    )
-    hi = []
-    for j in range(L):
-        op = "mad.hi.cc.u32" if j == 0 else ("madc.hi.u32" if j == L - 1 else "madc.hi.cc.u32")
-        hi.append(f"{op} {{o{j + 1}}}, {{i{j}}}, {{i{L}}}, {{o{j + 1}}};")
-    s.append(
-        _asm(
-            hi,
-            [f'"+r"(t[{j}])' for j in range(L + 1)],
-            [f'"r"(a[{j}])' for j in range(L)] + ['"r"(b[i])'],
-        ).replace("\n    ", "\n      ").replace("    asm", "      asm", 1)
-    )
-    s.append("      }\n")
-    s.append("      const uint32_t m = t[0] * np;\n")
-    # t += m * p: low halves (t[0] becomes 0), carry into t[L], t[L+1]
-    lo = []
-    for j in range(L):
-        op = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
-        lo.append(f"{op} {{o{j}}}, {{i{L}}}, {{i{j}}}, {{o{j}}};")
-    lo.append(f"addc.cc.u32 {{o{L}}}, {{o{L}}}, 0;")
-    lo.append(f"addc.u32 {{o{L + 1}}}, 0, 0;")
-    s.append(
-        _asm(
-            lo,
-            [f'"+r"(t[{j}])' for j in range(L + 1)] + [f'"=&r"(t[{L + 1}])'],
-            [f'"r"(p[{j}])' for j in range(L)] + ['"r"(m)'],
-        ).replace("\n    ", "\n      ").replace("    asm", "      asm", 1)
-    )
-    hi = []
-    for j in range(L):
-        op = "mad.hi.cc.u32" if j == 0 else "madc.hi.cc.u32"
-        hi.append(f"{op} {{o{j + 1}}}, {{i{L}}}, {{i{j}}}, {{o{j + 1}}};")
-    hi.append(f"addc.u32 {{o{L + 1}}}, {{o{L + 1}}}, 0;")
-    s.append(
-        _asm(
-            hi,
-            [f'"+r"(t[{j}])' for j in range(L + 2)],
-            [f'"r"(p[{j}])' for j in range(L)] + ['"r"(m)'],
-        ).replace("\n    ", "\n      ").replace("    asm", "      asm", 1)
-    )
-    s.append("#pragma unroll\n")
-    s.append(f"      for (int j = 0; j <= {L}; ++j) t[j] = t[j + 1];\n")
-    s.append("    }\n")
+        A.op(f"{op} {phys[j + 1]}, {{}}, {{}}, {phys[j + 1]};", f"a{j}", "b0")
+    for i in range(L):
+        if i > 0:
+            for j in range(L):
+                op = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
+                A.op(f"{op} {phys[j]}, {{}}, {{}}, {phys[j]};", f"a{j}", f"b{i}")
+            A.op(f"addc.u32 {phys[L]}, {phys[L]}, 0;")
+            for j in range(L):
+                op = "mad.hi.cc.u32" if j == 0 else ("madc.hi.u32" if j == L - 1 else "madc.hi.cc.u32")
+                A.op(f"{op} {phys[j + 1]}, {{}}, {{}}, {phys[j + 1]};", f"a{j}", f"b{i}")
+        A.op(f"mul.lo.u32 m, {phys[0]}, {{}};", "np")
+        for j in range(L):
+            op = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
+            A.op(f"{op} {phys[j]}, m, {{}}, {phys[j]};", f"p{j}")
+        A.op(f"addc.cc.u32 {phys[L]}, {phys[L]}, 0;")
+        A.op(f"addc.u32 {phys[L + 1]}, 0, 0;")
+        for j in range(L):
+            op = "mad.hi.cc.u32" if j == 0 else "madc.hi.cc.u32"
+            A.op(f"{op} {phys[j + 1]}, m, {{}}, {phys[j + 1]};", f"p{j}")
+        A.op(f"addc.u32 {phys[L + 1]}, {phys[L + 1]}, 0;")
+        phys = phys[1:] + phys[:1]  # t >>= 32 by renaming: the old t[0] (now zero) becomes t[L+1]
     # final conditional subtraction: t[0..L] < 2p
-    s.append(f"    uint32_t d[{L}], bw;\n")
-    sub = []
     for j in range(L):
         op = "sub.cc.u32" if j == 0 else "subc.cc.u32"
-        sub.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L + 1 + j}}};")
-    sub.append(f"subc.u32 {{o{L}}}, {{i{L}}}, 0;")
-    s.append(
-        _asm(
-            sub,
-            [f'"=&r"(d[{j}])' for j in range(L)] + ['"=&r"(bw)'],
-            [f'"r"(t[{j}])' for j in range(L + 1)] + [f'"r"(p[{j}])' for j in range(L)],
-        )
-    )
-    s.append("#pragma unroll\n")
-    s.append(f"    for (int j = 0; j < {L}; ++j) r[j] = bw ? t[j] : d[j];\n")
-    s.append("}\n\n")
-    return "".join(s)
+        A.op(f"{op} d{j}, {phys[j]}, {{}};", f"p{j}")
+    A.op(f"subc.u32 bw, {phys[L]}, 0;")
+    A.op("setp.ne.u32 keep, bw, 0;")
+    for j in range(L):
+        A.op(f"selp.b32 {{}}, {phys[j]}, d{j}, keep;", f"r{j}")
+    return head + A.render() + "}\n\n"
 
 
 def gen_add(L: int) -> str:
     """r = a + b mod p for a, b < p: add chain, trial subtraction, select."""
-    s = [
+    head = (
         f"template <> __device__ __forceinline__ void ptx_add_mod<{L}>(uint32_t (&r)[{L}], "
-        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}]) {{\n",
-        f"    uint32_t s[{L}], d[{L}], c, bw;\n",
-    ]
-    lines = []
+        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}]) {{\n"
+    )
+    outs = [(f"r{j}", f"r[{j}]") for j in range(L)]
+    ins = [(f"a{j}", f"a[{j}]") for j in range(L)] + [(f"b{j}", f"b[{j}]") for j in range(L)]
+    ins += [(f"p{j}", f"p[{j}]") for j in range(L)]
+    A = Asm(outs, ins)
+    A.locals_u32 = [f"s{j}" for j in range(L)] + [f"d{j}" for j in range(L)] + ["c", "bw"]
+    A.locals_pred = ["keep"]
     for j in range(L):
         op = "add.cc.u32" if j == 0 else "addc.cc.u32"
-        lines.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L + j}}};")
-    lines.append(f"addc.u32 {{o{L}}}, 0, 0;")
-    s.append(
-        _asm(
-            lines,
-            [f'"=&r"(s[{j}])' for j in range(L)] + ['"=&r"(c)'],
-            [f'"r"(a[{j}])' for j in range(L)] + [f'"r"(b[{j}])' for j in range(L)],
-        )
-    )
-    lines = []
+        A.op(f"{op} s{j}, {{}}, {{}};", f"a{j}", f"b{j}")
+    A.op("addc.u32 c, 0, 0;")
     for j in range(L):
         op = "sub.cc.u32" if j == 0 else "subc.cc.u32"
-        lines.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L + 1 + j}}};")
-    lines.append(f"subc.u32 {{o{L}}}, {{i{L}}}, 0;")
-    s.append(
-        _asm(
-            lines,
-            [f'"=&r"(d[{j}])' for j in range(L)] + ['"=&r"(bw)'],
-            [f'"r"(s[{j}])' for j in range(L)] + ['"r"(c)'] + [f'"r"(p[{j}])' for j in range(L)],
-        )
-    )
-    s.append("#pragma unroll\n")
-    s.append(f"    for (int j = 0; j < {L}; ++j) r[j] = bw ? s[j] : d[j];\n")
-    s.append("}\n\n")
-    return "".join(s)
+        A.op(f"{op} d{j}, s{j}, {{}};", f"p{j}")
+    A.op("subc.u32 bw, c, 0;")
+    A.op("setp.ne.u32 keep, bw, 0;")
+    for j in range(L):
+        A.op(f"selp.b32 {{}}, s{j}, d{j}, keep;", f"r{j}")
+    return head + A.render() + "}\n\n"
 
 
 def gen_sub(L: int) -> str:
     """r = a - b mod p for a, b < p: subtract chain, add p back under the borrow mask."""
-    s = [
+    head = (
         f"template <> __device__ __forceinline__ void ptx_sub_mod<{L}>(uint32_t (&r)[{L}], "
-        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}]) {{\n",
-        f"    uint32_t d[{L}], mask, q[{L}];\n",
-    ]
-    lines = []
+        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}]) {{\n"
+    )
+    outs = [(f"r{j}", f"r[{j}]") for j in range(L)]
+    ins = [(f"a{j}", f"a[{j}]") for j in range(L)] + [(f"b{j}", f"b[{j}]") for j in range(L)]
+    ins += [(f"p{j}", f"p[{j}]") for j in range(L)]
+    A = Asm(outs, ins)
+    A.locals_u32 = [f"d{j}" for j in range(L)] + [f"q{j}" for j in range(L)] + ["mask"]
     for j in range(L):
         op = "sub.cc.u32" if j == 0 else "subc.cc.u32"
-        lines.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L + j}}};")
-    lines.append(f"subc.u32 {{o{L}}}, 0, 0;")
-    s.append(
-        _asm(
-            lines,
-            [f'"=&r"(d[{j}])' for j in range(L)] + ['"=&r"(mask)'],
-            [f'"r"(a[{j}])' for j in range(L)] + [f'"r"(b[{j}])' for j in range(L)],
-        )
-    )
-    s.append("#pragma unroll\n")
-    s.append(f"    for (int j = 0; j < {L}; ++j) q[j] = p[j] & mask;\n")
-    lines = []
+        A.op(f"{op} d{j}, {{}}, {{}};", f"a{j}", f"b{j}")
+    A.op("subc.u32 mask, 0, 0;")
     for j in range(L):
-        op = "add.cc.u32" if j == 0 else ("addc.u32" if j == L - 1 else "addc.cc.u32")
+        A.op(f"and.b32 q{j}, {{}}, mask;", f"p{j}")
+    for j in range(L):
         if L == 1:
             op = "add.u32"
-        lines.append(f"{op} {{o{j}}}, {{i{j}}}, {{i{L + j}}};")
-    s.append(
-        _asm(
-            lines,
-            [f'"=&r"(r[{j}])' for j in range(L)],
-            [f'"r"(d[{j}])' for j in range(L)] + [f'"r"(q[{j}])' for j in range(L)],
-        )
-    )
-    s.append("}\n\n")
-    return "".join(s)
+        else:
+            op = "add.cc.u32" if j == 0 else ("addc.u32" if j == L - 1 else "addc.cc.u32")
+        A.op(f"{op} {{}}, d{j}, q{j};", f"r{j}")
+    return head + A.render() + "}\n\n"
 
 
 def generate() -> str:
     parts = [
         "// GENERATED by gen_field_ptx.py -- do not edit by hand.\n",
-        "// Inline-PTX carry chains of the field arithmetic for L = 1, 2, 4, 8 limbs.\n",
+        "// Inline-PTX carry chains of the field arithmetic for L = 1, 2, 4, 8 limbs; one asm\n",
+        "// statement per operation, intermediates in statement-local registers.\n",
         "#pragma once\n#include <cstdint>\n\n",
         "template <int L> __device__ __forceinline__ void ptx_mont_mul(uint32_t (&r)[L], "
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",

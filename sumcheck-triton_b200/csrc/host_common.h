@@ -131,11 +131,55 @@ inline int timing_collect(sc_ctx* ctx) {
   return SC_OK;
 }
 
-template <int L>
-inline int set_kernel_attrs() {
-  SC_CUDA(cudaFuncSetAttribute(round_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+// ---- compile-time instantiations: limb count L, field kind K, degree class DMAX ----
+
+inline int degree_class(int d) { return d <= 2 ? 2 : (d <= 4 ? 4 : 7); }
+
+inline int field_kind(const uint32_t* p, int L) {
+  return (L == 2 && p[0] == 1u && p[1] == 0xFFFFFFFFu) ? kFieldGoldilocks : kFieldGeneric;
+}
+
+// Calls Fn<L, K, DMAX>::run(args...) for the runtime (L, K, DMAX class).
+template <template <int, int, int> class Fn, int L, int K, typename... Args>
+inline int dispatch_degree(int dclass, Args&&... args) {
+  switch (dclass) {
+    case 2: return Fn<L, K, 2>::run(args...);
+    case 4: return Fn<L, K, 4>::run(args...);
+    default: return Fn<L, K, 7>::run(args...);
+  }
+}
+
+template <template <int, int, int> class Fn, typename... Args>
+inline int dispatch(int L, int K, int dclass, Args&&... args) {
+  switch (L) {
+    case 1: return dispatch_degree<Fn, 1, kFieldGeneric>(dclass, args...);
+    case 2:
+      return K == kFieldGoldilocks ? dispatch_degree<Fn, 2, kFieldGoldilocks>(dclass, args...)
+                                   : dispatch_degree<Fn, 2, kFieldGeneric>(dclass, args...);
+    case 4: return dispatch_degree<Fn, 4, kFieldGeneric>(dclass, args...);
+    default: return dispatch_degree<Fn, 8, kFieldGeneric>(dclass, args...);
+  }
+}
+
+// Calls Fn for every instantiation (set-up of kernel attributes).
+template <template <int, int, int> class Fn>
+inline int for_each_instance() {
+  const int combos[5][2] = {{1, kFieldGeneric}, {2, kFieldGeneric}, {2, kFieldGoldilocks}, {4, kFieldGeneric}, {8, kFieldGeneric}};
+  for (const auto& c : combos)
+    for (int dc : {2, 4, 7}) {
+      const int rc = dispatch<Fn>(c[0], c[1], dc);
+      if (rc) return rc;
+    }
   return SC_OK;
 }
+
+template <int L, int K, int D>
+struct SetRoundAttrs {
+  static int run() {
+    SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    return SC_OK;
+  }
+};
 
 // Montgomery image of a small non-negative integer.
 inline void mont_small(const HostField& hf, const uint32_t* r2, uint64_t v, uint32_t* out) {
@@ -174,6 +218,20 @@ inline bool cios_bound_holds(const HostField& hf) {
   return x[L + 1] == 0 && c == 0;
 }
 
+// Instruction-count estimates of one product and one modular add (for the choices below).
+inline int mul_cost(int L, int K) { return K == kFieldGoldilocks ? 16 : (L == 1 ? 10 : 4 * L * L + 8 * L); }
+inline int add_cost(int L) { return 3 * L + 4; }
+
+// Whether a term of length len in an expression of degree d is cheaper evaluated at points
+// 0..len and extrapolated by forward differences than evaluated at every point 0..d.
+inline bool extrapolate_term(int len, int d, int L, int K) {
+  if (len >= d) return false;
+  const int m = mul_cost(L, K), a = add_cost(L);
+  const int direct = (len - 1) * (d + 1) * m + len * d * a;
+  const int extrap = (len - 1) * (len + 1) * m + len * len * a + (len * (len + 1) / 2 + d * len) * a;
+  return extrap < direct;
+}
+
 template <int L>
 inline void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
   std::memset(&E, 0, sizeof(E));
@@ -181,7 +239,9 @@ inline void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
   E.num_terms = ex.num_terms;
   E.degree = ex.degree;
   const HostField& hf = f.hf;
-  const int mul_cost = 4 * L * L + 8 * L, add_cost = 3 * L + 3;
+  const int K = field_kind(hf.p, L);
+  for (int i = 0; i < ex.num_terms; ++i) E.term_extrap[i] = extrapolate_term(ex.lens[i], ex.degree, L, K) ? 1 : 0;
+  const int mul_cost = ::sc_host::mul_cost(L, K), add_cost = ::sc_host::add_cost(L);
   for (int i = 0; i < ex.num_terms; ++i) {
     E.term_len[i] = static_cast<uint8_t>(ex.lens[i]);
     E.term_off[i] = static_cast<uint8_t>(ex.offs[i]);
@@ -226,7 +286,7 @@ inline void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
 }
 
 struct StateOffsets {
-  size_t counter, status, checksum, polys, chals, finals, claim0, total_words;
+  size_t counter, status, checksum, polys, chals, finals, claim0, claim, total_words;
 };
 
 inline StateOffsets state_offsets(int n, int K, int L) {
@@ -238,7 +298,8 @@ inline StateOffsets state_offsets(int n, int K, int L) {
   o.chals = o.polys + static_cast<size_t>(n) * kMaxPoints * L;
   o.finals = o.chals + static_cast<size_t>(n) * L;
   o.claim0 = o.finals + static_cast<size_t>(1 + K) * L;
-  o.total_words = o.claim0 + L;
+  o.claim = o.claim0 + L;
+  o.total_words = o.claim + L;
   return o;
 }
 

@@ -39,11 +39,6 @@ namespace {
 std::mutex g_noalloc_mu;
 uint32_t* g_noalloc_ptr[kMaxDevices] = {};
 
-template <int L>
-int noalloc_kernel_attrs() {
-  SC_CUDA(cudaFuncSetAttribute(round_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-  return SC_OK;
-}
 
 // Device address of the scratch array on `device` (the device must be current).
 int noalloc_scratch(int device, uint32_t** out) {
@@ -54,10 +49,8 @@ int noalloc_scratch(int device, uint32_t** out) {
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return fail(SC_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", device, cudaGetErrorString(e));
-    int rc;
-    if ((rc = noalloc_kernel_attrs<1>()) || (rc = noalloc_kernel_attrs<2>()) || (rc = noalloc_kernel_attrs<4>()) ||
-        (rc = noalloc_kernel_attrs<8>()))
-      return rc;
+    const int rc = for_each_instance<SetRoundAttrs>();
+    if (rc) return rc;
     g_noalloc_ptr[device] = static_cast<uint32_t*>(p);
   }
   *out = g_noalloc_ptr[device];
@@ -66,40 +59,43 @@ int noalloc_scratch(int device, uint32_t** out) {
 
 constexpr size_t align64(size_t w) { return (w + 63) & ~size_t{63}; }  // 256-byte steps
 
-template <int L>
-int noalloc_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables, int mode,
-                 const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch, uint32_t* out_finals,
-                 uint32_t* out_claim0, uint64_t* out_checksum) {
-  const int K = ex->num_vars, d = ex->degree;
+constexpr uint64_t kNoAllocSkip1MinPairs = uint64_t{1} << 12;
+
+template <int L, int K, int DMAX>
+struct NoallocRun {
+static int run(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables, int mode,
+               const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch, uint32_t* out_finals,
+               uint32_t* out_claim0, uint64_t* out_checksum) {
+  const int K_ = ex->num_vars, d = ex->degree;
   const uint64_t N = uint64_t{1} << n;
   uint32_t* base = nullptr;
   int rc;
   if ((rc = noalloc_scratch(ctx->device, &base))) return rc;  // first call on a device: set-up
-  int threads = kBlock;
-  const int per_thread = round_smem_words_per_thread(K, L) * 4;
+  int threads = kernel_threads(L);
+  const int per_thread = round_smem_words_per_thread(K_, L) * 4;
   while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
   const size_t smem = static_cast<size_t>(threads) * per_thread;
   int bps = 0;
-  SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, round_kernel<L>, threads, smem));
-  if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K, L);
+  SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, round_kernel<L, K, DMAX>, threads, smem));
+  if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K_, L);
   const uint64_t grid_max = std::min<uint64_t>(static_cast<uint64_t>(bps) * ctx->sm_count, kNoAllocMaxBlocks);
 
   // carve the scratch array: field constants, proof state, partials, fold A, fold B
-  const StateOffsets so = state_offsets(n, K, L);
+  const StateOffsets so = state_offsets(n, K_, L);
   const size_t w_fc = 0;
   const size_t w_state = w_fc + align64(sizeof(FieldConsts) / 4);
   const size_t w_part = w_state + align64(so.total_words);
   const size_t w_a = w_part + align64(grid_max * kMaxPoints * L);
-  const size_t w_b = w_a + align64(n >= 2 ? static_cast<size_t>(K) * L * (N / 2) : 0);
-  const size_t w_end = w_b + align64(n >= 3 ? static_cast<size_t>(K) * L * (N / 4) : 0);
+  const size_t w_b = w_a + align64(n >= 2 ? static_cast<size_t>(K_) * L * (N / 2) : 0);
+  const size_t w_end = w_b + align64(n >= 3 ? static_cast<size_t>(K_) * L * (N / 4) : 0);
   if (w_end * 4 > kNoAllocScratchBytes)
     return fail(SC_ERR_UNSUPPORTED,
                 "sc_prove_noalloc: this proof (%d tables, %d limbs, 2^%d entries) needs %zu bytes of scratch; "
                 "the no-allocation scratch holds %zu bytes (use sc_prove)",
-                K, L, n, w_end * 4, kNoAllocScratchBytes);
+                K_, L, n, w_end * 4, kNoAllocScratchBytes);
   ExprDev E;
   build_expr_dev<L>(*ex, *f, E);
-  FieldParams<L> F;
+  FieldParams<L, K> F;
   for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
   F.np = f->hf.np;
 
@@ -122,10 +118,13 @@ int noalloc_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const
   A.st.chals = st + so.chals;
   A.st.finals = st + so.finals;
   A.st.claim0 = st + so.claim0;
+  A.st.claim = st + so.claim;
   const uint32_t* prev = tables;
   for (int j = 0; j < n; ++j) {
     A.round = j;
     A.pairs = N >> (j + 1);
+    A.skip1 = (j >= 1 && (N >> (j + 1)) >= kNoAllocSkip1MinPairs) ? 1 : 0;
+    A.want_claim = (j + 1 < n && (N >> (j + 2)) >= kNoAllocSkip1MinPairs) ? 1 : 0;
     if (j == 0) {
       A.fold = 0;
       A.src = tables;
@@ -140,7 +139,7 @@ int noalloc_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const
     }
     const uint64_t want = (A.pairs + threads - 1) / threads;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
-    round_kernel<L><<<grid, threads, smem, ctx->stream>>>(A, E, F);
+    round_kernel<L, K, DMAX><<<grid, threads, smem, ctx->stream>>>(A, E, F);
     SC_CUDA(cudaGetLastError());
   }
   // results straight into the caller's arrays (no staging buffer)
@@ -153,7 +152,7 @@ int noalloc_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const
   if (out_ch)
     SC_CUDA(cudaMemcpyAsync(out_ch, st + so.chals, static_cast<size_t>(n) * L * 4, cudaMemcpyDeviceToHost, ctx->stream));
   if (out_finals)
-    SC_CUDA(cudaMemcpyAsync(out_finals, st + so.finals, static_cast<size_t>(1 + K) * L * 4, cudaMemcpyDeviceToHost,
+    SC_CUDA(cudaMemcpyAsync(out_finals, st + so.finals, static_cast<size_t>(1 + K_) * L * 4, cudaMemcpyDeviceToHost,
                             ctx->stream));
   if (out_claim0) SC_CUDA(cudaMemcpyAsync(out_claim0, st + so.claim0, L * 4, cudaMemcpyDeviceToHost, ctx->stream));
   if (out_checksum) SC_CUDA(cudaMemcpyAsync(out_checksum, st + so.checksum, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -161,6 +160,7 @@ int noalloc_impl(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const
   if (status) return fail(SC_ERR_DEVICE, "device status %u", status);
   return SC_OK;
 }
+};
 
 }  // namespace
 
@@ -177,10 +177,7 @@ extern "C" int sc_prove_noalloc(sc_ctx* ctx, const sc_field* field, const sc_exp
     return fail(SC_ERR_INVALID, "explicit challenge mode needs explicit_challenges");
   if (reinterpret_cast<uintptr_t>(tables_dev) % 16) return fail(SC_ERR_INVALID, "tables_dev must be 16-byte aligned");
   SC_CUDA(cudaSetDevice(ctx->device));
-  switch (field->hf.L) {
-    case 1: return noalloc_impl<1>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    case 2: return noalloc_impl<2>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    case 4: return noalloc_impl<4>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-    default: return noalloc_impl<8>(ctx, field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
-  }
+  return dispatch<NoallocRun>(field->hf.L, field_kind(field->hf.p, field->hf.L), degree_class(expr->degree), ctx,
+                              field, expr, num_rounds, tables_dev, challenge_mode, explicit_challenges,
+                              out_round_polys, out_challenges, out_finals, out_claim0, out_checksum);
 }

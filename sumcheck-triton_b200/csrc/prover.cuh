@@ -8,16 +8,21 @@
 //      reference field_sumcheck.cu:677-694, fused into this round's read);
 //   2. evaluate: extends every table's pair to t = 0..d (v(t) = v(t-1) + (o - e); reference
 //      field_sumcheck.cu:326-348) and evaluates the constraint at each point
-//      (field_sumcheck.cu:389-590), accumulating d+1 sums per thread;
+//      (field_sumcheck.cu:389-590), accumulating d+1 sums per thread (see eval_pair for the
+//      exact-arithmetic shortcuts: extrapolated low-degree terms, g(1) from the claim);
 //   3. reduce: warp shuffles, then shared memory, then one partial per block in global
 //      memory; the last block to finish (atomic ticket) sums the partials -- a single-pass
 //      grid reduction in place of the reference's log-depth launch tree
 //      (field_sumcheck.cu:635-675, :996-1010);
 //   4. finalise (last block only): stores g_j(0..d), adds the round's checksum, derives r_j
-//      by SHA3 over the round polynomial on the device (field_sumcheck.cu:857-907) and, in
-//      the last round, the final claim g_{n-1}(r_{n-1}) and the folded values f_k(r).
+//      by SHA3 over the round polynomial on the device (field_sumcheck.cu:857-907), and when
+//      needed g_j(r_j) (the next round's claim) and, in the last round, the final claim and
+//      the folded values f_k(r).
 //
 // Tables are limb-planar: table k, limb l is the u32 plane at (k * L + l) * len.
+// Kernels are templates over the limb count L, the field kind K (a special reduction for
+// Goldilocks) and DMAX, the largest degree the launch handles (register arrays of DMAX + 1
+// points; the host picks the smallest class >= the expression's degree).
 #pragma once
 #include <cstdint>
 
@@ -34,7 +39,8 @@ constexpr int kMaxRounds = 40;
 enum ChallengeMode : int32_t { kChallengeSha3 = 0, kChallengeFixed = 1, kChallengeExplicit = 2 };
 
 // Coefficient handling per term: +1 / -1 are an add / a subtract; other small values an
-// addition chain; anything else a product with the coefficient's Montgomery image.
+// addition chain; anything else a product with the coefficient's Montgomery image. The
+// scaling is applied once per pair to the first factor (value and difference), not per point.
 enum CoeffKind : uint8_t { kCoeffPlus = 0, kCoeffMinus = 1, kCoeffSmall = 2, kCoeffMont = 3 };
 
 // Constants of one field that only the finalisation needs (device memory, per field).
@@ -60,6 +66,7 @@ struct ExprDev {
   uint8_t term_off[kMaxTerms];
   uint8_t flat[kMaxFlat];
   uint8_t coeff_kind[kMaxTerms];
+  uint8_t term_extrap[kMaxTerms];   // 1: evaluate points 0..len only, extrapolate the rest
   int32_t coeff_small[kMaxTerms];
   uint32_t coeff_mont[kMaxTerms][kMaxLimbs];
 };
@@ -73,6 +80,7 @@ struct ProofState {
   uint32_t* finals;      // [1 + K][L]: g_{n-1}(r_{n-1}), then f_k(r) for every table
   uint32_t* claim0;      // [L]
   uint32_t* status;      // nonzero on a device-detected error
+  uint32_t* claim;       // [L]: g_{j-1}(r_{j-1}), the claim round j's g(0) + g(1) must meet
 };
 
 struct RoundArgs {
@@ -84,6 +92,8 @@ struct RoundArgs {
   int32_t num_rounds;
   int32_t fold;
   int32_t mode;          // ChallengeMode
+  int32_t skip1;         // g(1) = claim - g(0) instead of evaluating point 1
+  int32_t want_claim;    // store g_j(r_j) for the next round
   uint32_t* partials;    // [gridDim.x][kMaxPoints][L]
   const FieldConsts* fc;
   ProofState st;
@@ -126,54 +136,153 @@ __device__ __forceinline__ void sm_put(uint32_t* sm, int slot, int tid, int nthr
   for (int l = 0; l < L; ++l) sm[(slot * L + l) * nthr + tid] = a.w[l];
 }
 
-// Evaluate the runtime expression on the point values held in shared memory.
-template <int L>
-__device__ __forceinline__ Fe<L> eval_expr(const ExprDev& E, const uint32_t* sv, int tid, int nthr,
-                                           const FieldParams<L>& F) {
-  Fe<L> total = fe_zero<L>();
+template <int L, int K>
+__device__ __forceinline__ Fe<L> add_or_sub(const Fe<L>& acc, const Fe<L>& x, bool neg, const FieldParams<L, K>& F) {
+  return neg ? fe_sub(acc, x, F) : fe_add(acc, x, F);
+}
+
+// One pair: acc[t] += expression at point t, for t = 0..d (t = 1 skipped when skip1).
+// The values and differences of every table are in shared memory (this thread's slots).
+//
+// A term of len factors is a polynomial of degree len in t. Evaluated at points 0..last
+// (last = d, or len when the host marked the term for extrapolation), each point costs len-1
+// products: the factors' values are stepped point to point by one addition of the
+// difference. An extrapolated term's points len+1..d come from its forward differences
+// (len(len+1)/2 subtractions, then len additions per step) -- exact, since the term is a
+// polynomial of degree len; the host marks a term only where that is cheaper than the
+// products it replaces. With skip1, point 1 of a directly evaluated term is never formed.
+template <int L, int K, int DMAX>
+__device__ __forceinline__ void eval_pair(const ExprDev& E, const uint32_t* sv, const uint32_t* sd, int tid, int nthr,
+                                          bool skip1, Fe<L> (&acc)[DMAX + 1], const FieldParams<L, K>& F) {
+  const int d = E.degree;
   for (int i = 0; i < E.num_terms; ++i) {
     const int off = E.term_off[i];
     const int len = E.term_len[i];
-    Fe<L> prod = sm_get<L>(sv, E.flat[off], tid, nthr);
-    for (int f = 1; f < len; ++f) prod = fe_mul(prod, sm_get<L>(sv, E.flat[off + f], tid, nthr), F);
-    switch (E.coeff_kind[i]) {
-      case kCoeffPlus:
-        total = fe_add(total, prod, F);
-        break;
-      case kCoeffMinus:
-        total = fe_sub(total, prod, F);
-        break;
-      case kCoeffSmall: {
+    const int kind = E.coeff_kind[i];
+    const bool extrap = E.term_extrap[i] != 0;
+    const int last = extrap ? len : d;
+    const bool skip_t1 = skip1 && !extrap;
+    const bool neg = kind == kCoeffMinus || (kind == kCoeffSmall && E.coeff_small[i] < 0);
+    Fe<L> prod[DMAX + 1];
+    {
+      const int k0 = E.flat[off];
+      Fe<L> v = sm_get<L>(sv, k0, tid, nthr);
+      Fe<L> df = sm_get<L>(sd, k0, tid, nthr);
+      if (kind == kCoeffSmall) {
         const int32_t c = E.coeff_small[i];
-        const Fe<L> s = fe_mul_small(prod, c < 0 ? -c : c, F);
-        total = c < 0 ? fe_sub(total, s, F) : fe_add(total, s, F);
-        break;
-      }
-      default: {
+        const uint32_t m = c < 0 ? static_cast<uint32_t>(-static_cast<int64_t>(c)) : static_cast<uint32_t>(c);
+        v = fe_mul_small(v, m, F);
+        df = fe_mul_small(df, m, F);
+      } else if (kind == kCoeffMont) {
         Fe<L> cm;
 #pragma unroll
         for (int l = 0; l < L; ++l) cm.w[l] = E.coeff_mont[i][l];
-        total = fe_add(total, fe_mul(prod, cm, F), F);
+        v = fe_mul(v, cm, F);
+        df = fe_mul(df, cm, F);
+      }
+#pragma unroll
+      for (int t = 0; t <= DMAX; ++t) {
+        if (t > last) break;
+        prod[t] = v;
+        if (t < last) v = fe_add(v, df, F);
+      }
+    }
+    for (int f = 1; f < len; ++f) {
+      const int k = E.flat[off + f];
+      Fe<L> v = sm_get<L>(sv, k, tid, nthr);
+      const Fe<L> df = sm_get<L>(sd, k, tid, nthr);
+#pragma unroll
+      for (int t = 0; t <= DMAX; ++t) {
+        if (t > last) break;
+        if (!(skip_t1 && t == 1)) prod[t] = fe_mul(prod[t], v, F);
+        if (t < last) v = fe_add(v, df, F);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t <= DMAX; ++t) {
+      if (t > last) break;
+      if (skip1 && t == 1) continue;
+      acc[t] = add_or_sub(acc[t], prod[t], neg, F);
+    }
+    if (extrap && len < d) {
+      // forward differences at 0, in place: prod[m] = Delta^m p(0)
+#pragma unroll
+      for (int m = 1; m <= DMAX; ++m) {
+        if (m > len) break;
+#pragma unroll
+        for (int t = DMAX; t >= 1; --t) {
+          if (t > len || t < m) continue;
+          prod[t] = fe_sub(prod[t], prod[t - 1], F);
+        }
+      }
+      // step forward: after s steps prod[0] = p(s)
+#pragma unroll
+      for (int s = 1; s <= DMAX; ++s) {
+        if (s > d) break;
+#pragma unroll
+        for (int m = 0; m < DMAX; ++m) {
+          if (m >= len) break;
+          prod[m] = fe_add(prod[m], prod[m + 1], F);
+        }
+        if (s > len && !(skip1 && s == 1)) acc[s] = add_or_sub(acc[s], prod[0], neg, F);
       }
     }
   }
-  return total;
+}
+
+// Folds (if fold) and evaluates pairs q = first, first + stride, ... < last, adding the
+// point sums into acc. sv / sd: this block's [K][L][nthr] shared arrays.
+template <int L, int K, int DMAX>
+__device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst, uint64_t src_len, bool fold,
+                                              const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
+                                              uint64_t first, uint64_t last, uint64_t stride, bool skip1,
+                                              Fe<L> (&acc)[DMAX + 1], const FieldParams<L, K>& F) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nv = E.num_vars;
+  for (uint64_t q = first; q < last; q += stride) {
+    for (int k = 0; k < nv; ++k) {
+      Fe<L> e, o;
+      if (fold) {
+        Fe<L> x0, x1, x2, x3;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          const uint4 v = __ldcs(reinterpret_cast<const uint4*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
+          x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
+        }
+        e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
+        o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
+        const uint64_t dst_len = src_len >> 1;
+#pragma unroll
+        for (int l = 0; l < L; ++l)
+          reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+      } else {
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          const uint2 v = __ldcs(reinterpret_cast<const uint2*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
+          e.w[l] = v.x; o.w[l] = v.y;
+        }
+      }
+      sm_put<L>(sv, k, tid, nthr, e);
+      sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
+    }
+    eval_pair<L, K, DMAX>(E, sv, sd, tid, nthr, skip1, acc, F);
+  }
 }
 
 // Reduce acc[0..d] over the block; the block sums land in red_out[t * L + l] (shared).
-template <int L>
-__device__ __forceinline__ void block_reduce(Fe<L> (&acc)[kMaxPoints], int d, uint32_t* scratch,
-                                             uint32_t* red_out, const FieldParams<L>& F) {
+template <int L, int K, int N>
+__device__ __forceinline__ void block_reduce(Fe<L> (&acc)[N], int d, uint32_t* scratch, uint32_t* red_out,
+                                             const FieldParams<L, K>& F) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
 #pragma unroll
-  for (int t = 0; t < kMaxPoints; ++t) {
+  for (int t = 0; t < N; ++t) {
     if (t > d) break;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc[t] = fe_add(acc[t], fe_shfl_down(acc[t], off), F);
   }
   if (lane == 0) {
 #pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) {
+    for (int t = 0; t < N; ++t) {
       if (t > d) break;
       st_fe<L>(scratch + (warp * kMaxPoints + t) * L, acc[t]);
     }
@@ -181,7 +290,7 @@ __device__ __forceinline__ void block_reduce(Fe<L> (&acc)[kMaxPoints], int d, ui
   __syncthreads();
   if (warp == 0) {
 #pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) {
+    for (int t = 0; t < N; ++t) {
       if (t > d) break;
       Fe<L> v = lane < nwarps ? ld_fe<L>(scratch + (lane * kMaxPoints + t) * L) : fe_zero<L>();
 #pragma unroll
@@ -192,19 +301,60 @@ __device__ __forceinline__ void block_reduce(Fe<L> (&acc)[kMaxPoints], int d, ui
   __syncthreads();
 }
 
+// Sums the partials of blocks/items [first, first + count) into g_sm[t * L + l] (block-wide).
+template <int L, int K, int N>
+__device__ __forceinline__ void reduce_partials(const uint32_t* partials, uint64_t first, uint64_t count, int d,
+                                                uint32_t* scratch, uint32_t* g_sm, const FieldParams<L, K>& F) {
+  Fe<L> acc[N];
+#pragma unroll
+  for (int t = 0; t < N; ++t) acc[t] = fe_zero<L>();
+  for (uint64_t b = threadIdx.x; b < count; b += blockDim.x) {
+    const uint32_t* pb = partials + (first + b) * kMaxPoints * L;
+#pragma unroll
+    for (int t = 0; t < N; ++t) {
+      if (t > d) break;
+      acc[t] = fe_add(acc[t], ld_fe_cg<L>(pb + t * L), F);
+    }
+  }
+  block_reduce<L, K, N>(acc, d, scratch, g_sm, F);
+}
+
 template <int L>
 __device__ __forceinline__ Fe<L> fc_get(const uint32_t* row) {
   return ld_fe<L>(row);
 }
 
-// Last block of a round: g_j is in g_sm[t * L + l]. Warp 0 does all of this.
-template <int L>
-__device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const FieldParams<L>& F,
-                               const uint32_t* g_sm, uint8_t* msg) {
+// g(r) for the polynomial with values g_sm[t] at t = 0..d (Lagrange form with the field's
+// precomputed weights); lane t < d + 1 forms one term, the warp sums them (all lanes call).
+template <int L, int K>
+__device__ __forceinline__ Fe<L> lagrange_at(const uint32_t* g_sm, int d, const Fe<L>& r, const FieldConsts& fc,
+                                             const FieldParams<L, K>& F) {
+  const int lane = threadIdx.x & 31;
+  Fe<L> term = fe_zero<L>();
+  if (lane <= d) {
+    term = fe_mul(ld_fe<L>(g_sm + lane * L), fc_get<L>(fc.lag[d][lane]), F);
+    for (int s = 0; s <= d; ++s)
+      if (s != lane) term = fe_mul(term, fe_sub(r, fc_get<L>(fc.pts[s]), F), F);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) term = fe_add(term, fe_shfl_down(term, off), F);
+  return fe_shfl(term, 0);
+}
+
+// Last block of a round: g_j is in g_sm[t * L + l] (point 1 still empty when skip1).
+// Warp 0 does all of this.
+template <int L, int K>
+__device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const FieldParams<L, K>& F, uint32_t* g_sm,
+                               uint8_t* msg) {
   const int lane = threadIdx.x & 31;
   const int d = E.degree;
   const int j = A.round;
   const FieldConsts& fc = *A.fc;
+  // 0. g(1) from the claim this round must meet
+  if (A.skip1) {
+    if (lane == 0) st_fe<L>(g_sm + L, fe_sub(ld_fe_cg<L>(A.st.claim), ld_fe<L>(g_sm), F));
+    __syncwarp();
+  }
   // 1. round polynomial and checksum
   for (int i = lane; i < (d + 1) * L; i += 32) A.st.polys[(j * kMaxPoints + i / L) * L + i % L] = g_sm[i];
   if (lane == 0) {
@@ -254,19 +404,16 @@ __device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const Field
     r = fc_get<L>(fc.one);
     if (lane == 0) st_fe<L>(A.st.chals + j * L, r);
   } else {
-    r = ld_fe<L>(A.st.chals + j * L);
+    r = ld_fe_cg<L>(A.st.chals + j * L);
   }
-  // 3. last round: final claim g(r) by Lagrange interpolation, and f_k(r) per table
-  if (j == A.num_rounds - 1) {
-    Fe<L> term = fe_zero<L>();
-    if (lane <= d) {
-      term = fe_mul(ld_fe<L>(g_sm + lane * L), fc_get<L>(fc.lag[d][lane]), F);
-      for (int s = 0; s <= d; ++s)
-        if (s != lane) term = fe_mul(term, fe_sub(r, fc_get<L>(fc.pts[s]), F), F);
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) term = fe_add(term, fe_shfl_down(term, off), F);
-    if (lane == 0) st_fe<L>(A.st.finals, term);
+  // 3. g_j(r_j): the next round's claim, and in the last round the final claim
+  const bool last_round = j == A.num_rounds - 1;
+  if (A.want_claim || last_round) {
+    const Fe<L> gr = lagrange_at<L, K>(g_sm, d, r, fc, F);
+    if (lane == 0) st_fe<L>(last_round ? A.st.finals : A.st.claim, gr);
+  }
+  // 4. last round: f_k(r) per table
+  if (last_round) {
     const uint32_t* tab = A.fold ? A.dst : A.src;  // T_{n-1}: 2 entries per plane
     for (int k = lane; k < E.num_vars; k += 32) {
       Fe<L> e, o;
@@ -284,74 +431,15 @@ __device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const Field
 // Dynamic shared memory per thread: values and differences of every table.
 __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { return 2 * K * L; }
 
-// Folds (if A.fold) and evaluates pairs q = first, first + stride, ... < last, adding the
-// d+1 point sums into acc. sv / sd: this block's [K][L][nthr] shared arrays.
-template <int L>
-__device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst, uint64_t src_len, bool fold,
-                                              const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
-                                              uint64_t first, uint64_t last, uint64_t stride,
-                                              Fe<L> (&acc)[kMaxPoints], const FieldParams<L>& F) {
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int K = E.num_vars, d = E.degree;
-  for (uint64_t q = first; q < last; q += stride) {
-    for (int k = 0; k < K; ++k) {
-      Fe<L> e, o;
-      if (fold) {
-        Fe<L> x0, x1, x2, x3;
-#pragma unroll
-        for (int l = 0; l < L; ++l) {
-          const uint4 v = __ldcs(reinterpret_cast<const uint4*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
-          x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
-        }
-        e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
-        o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
-        const uint64_t dst_len = src_len >> 1;
-#pragma unroll
-        for (int l = 0; l < L; ++l)
-          reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
-      } else {
-#pragma unroll
-        for (int l = 0; l < L; ++l) {
-          const uint2 v = __ldcs(reinterpret_cast<const uint2*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
-          e.w[l] = v.x; o.w[l] = v.y;
-        }
-      }
-      sm_put<L>(sv, k, tid, nthr, e);
-      sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
-    }
-#pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) {
-      if (t > d) break;
-      if (t > 0) {
-        for (int k = 0; k < K; ++k)
-          sm_put<L>(sv, k, tid, nthr, fe_add(sm_get<L>(sv, k, tid, nthr), sm_get<L>(sd, k, tid, nthr), F));
-      }
-      acc[t] = fe_add(acc[t], eval_expr<L>(E, sv, tid, nthr, F), F);
-    }
-  }
-}
+// Launch shape per limb count: 8-limb kernels hold (DMAX + 1) x 8-word point arrays per
+// thread, so they run 128-thread blocks and ask the compiler for at least 3 blocks per SM
+// (<= 170 registers); smaller fields run 256-thread blocks.
+__host__ __device__ constexpr int kernel_threads(int L) { return L >= 8 ? 128 : 256; }
+__host__ __device__ constexpr int kernel_min_blocks(int L) { return L >= 8 ? 3 : 1; }
 
-// Sums the partials of blocks/items [first, first + count) into g_sm[t * L + l] (block-wide).
-template <int L>
-__device__ __forceinline__ void reduce_partials(const uint32_t* partials, uint64_t first, uint64_t count, int d,
-                                                uint32_t* scratch, uint32_t* g_sm, const FieldParams<L>& F) {
-  Fe<L> acc[kMaxPoints];
-#pragma unroll
-  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
-  for (uint64_t b = threadIdx.x; b < count; b += blockDim.x) {
-    const uint32_t* pb = partials + (first + b) * kMaxPoints * L;
-#pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) {
-      if (t > d) break;
-      acc[t] = fe_add(acc[t], ld_fe_cg<L>(pb + t * L), F);
-    }
-  }
-  block_reduce<L>(acc, d, scratch, g_sm, F);
-}
-
-template <int L>
-__global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const ExprDev E,
-                                                    const FieldParams<L> F) {
+template <int L, int K, int DMAX>
+__global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
+    round_kernel(const RoundArgs A, const ExprDev E, const FieldParams<L, K> F) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
   __shared__ __align__(16) uint8_t msg[3 * 136];
@@ -363,18 +451,18 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
   uint32_t* sv = smem;                           // [K][L][nthr] values at the current point
   uint32_t* sd = smem + E.num_vars * L * nthr;   // [K][L][nthr] differences o - e
 
-  Fe<L> acc[kMaxPoints];
+  Fe<L> acc[DMAX + 1];
 #pragma unroll
-  for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+  for (int t = 0; t <= DMAX; ++t) acc[t] = fe_zero<L>();
   Fe<L> r_prev = fe_zero<L>();
   if (A.fold) r_prev = ld_fe_cg<L>(A.st.chals + (A.round - 1) * L);
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * nthr;
-  process_pairs<L>(A.src, A.dst, A.src_len, A.fold != 0, r_prev, E, sv, sd,
-                   static_cast<uint64_t>(blockIdx.x) * nthr + tid, A.pairs, stride, acc, F);
+  process_pairs<L, K, DMAX>(A.src, A.dst, A.src_len, A.fold != 0, r_prev, E, sv, sd,
+                            static_cast<uint64_t>(blockIdx.x) * nthr + tid, A.pairs, stride, A.skip1 != 0, acc, F);
 
   // block partial -> global; the last block reduces all partials
   __syncthreads();
-  block_reduce<L>(acc, d, smem, g_sm, F);
+  block_reduce<L, K, DMAX + 1>(acc, d, smem, g_sm, F);
   for (int i = tid; i < (d + 1) * L; i += nthr) A.partials[static_cast<uint64_t>(blockIdx.x) * kMaxPoints * L + i] = g_sm[i];
   __threadfence();
   __syncthreads();
@@ -382,8 +470,8 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  reduce_partials<L>(A.partials, 0, gridDim.x, d, smem, g_sm, F);
-  if (tid < 32) finalize_round<L>(A, E, F, g_sm, msg);
+  reduce_partials<L, K, DMAX + 1>(A.partials, 0, gridDim.x, d, smem, g_sm, F);
+  if (tid < 32) finalize_round<L, K>(A, E, F, g_sm, msg);
   if (tid == 0) {
     __threadfence();
     *A.st.counter = 0;
@@ -392,17 +480,17 @@ __global__ void __launch_bounds__(256) round_kernel(const RoundArgs A, const Exp
 
 // ------------------------------------------------------------------------------ batched
 //
-// Many independent proofs advance one round per "tick". A tick is one launch per field
-// class: a persistent kernel whose blocks pull (proof round, tile of pairs) items from a
-// device work queue (an atomic counter over the tick's item list). Every item leaves one
-// partial; the block that finishes the last item of a proof's round (per-proof atomic
-// ticket) reduces that proof's partials and finalises its round -- SHA3 challenge
-// included -- while the other blocks go on with other proofs' items.
+// Many independent proofs advance one round per "tick". A tick is one launch per (field,
+// degree class): a persistent kernel whose blocks pull (proof round, tile of pairs) items
+// from a device work queue (an atomic counter over the tick's item list). Every item leaves
+// one partial; the block that finishes the last item of a proof's round (per-proof atomic
+// ticket) reduces that proof's partials and finalises its round -- SHA3 challenge included
+// -- while the other blocks go on with other proofs' items.
 
 struct BatchRound {
-  RoundArgs args;      // this proof's round (src/dst/len/pairs/round/fold/mode/fc/state)
+  RoundArgs args;      // this proof's round (src/dst/len/pairs/round/fold/mode/flags/fc/state)
   int32_t expr;        // index into the batch's expression table
-  int32_t first_item;  // this round's items: [first_item, first_item + num_items)
+  int32_t first_item;  // this round's items: [first_item, first_item + num_items) of the tick
   int32_t num_items;
   int32_t pad;
 };
@@ -424,8 +512,9 @@ struct BatchTickArgs {
   uint32_t* partials;  // [num_items][kMaxPoints][L], indexed by item
 };
 
-template <int L>
-__global__ void __launch_bounds__(256) batch_round_kernel(const BatchTickArgs T, const FieldParams<L> F) {
+template <int L, int K, int DMAX>
+__global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
+    batch_round_kernel(const BatchTickArgs T, const FieldParams<L, K> F) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
   __shared__ __align__(16) uint8_t msg[3 * 136];
@@ -452,17 +541,17 @@ __global__ void __launch_bounds__(256) batch_round_kernel(const BatchTickArgs T,
       if (tid == 0) cur_expr = R.expr;
     }
     const int d = E.degree;
-    Fe<L> acc[kMaxPoints];
+    Fe<L> acc[DMAX + 1];
 #pragma unroll
-    for (int t = 0; t < kMaxPoints; ++t) acc[t] = fe_zero<L>();
+    for (int t = 0; t <= DMAX; ++t) acc[t] = fe_zero<L>();
     Fe<L> r_prev = fe_zero<L>();
     if (R.args.fold) r_prev = ld_fe_cg<L>(R.args.st.chals + (R.args.round - 1) * L);
     uint32_t* sv = smem;
     uint32_t* sd = smem + E.num_vars * L * nthr;
-    process_pairs<L>(R.args.src, R.args.dst, R.args.src_len, R.args.fold != 0, r_prev, E, sv, sd,
-                     I.start + tid, I.start + I.count, nthr, acc, F);
+    process_pairs<L, K, DMAX>(R.args.src, R.args.dst, R.args.src_len, R.args.fold != 0, r_prev, E, sv, sd,
+                              I.start + tid, I.start + I.count, nthr, R.args.skip1 != 0, acc, F);
     __syncthreads();
-    block_reduce<L>(acc, d, smem, g_sm, F);
+    block_reduce<L, K, DMAX + 1>(acc, d, smem, g_sm, F);
     for (int i = tid; i < (d + 1) * L; i += nthr) T.partials[static_cast<uint64_t>(it) * kMaxPoints * L + i] = g_sm[i];
     __threadfence();
     __syncthreads();
@@ -470,8 +559,8 @@ __global__ void __launch_bounds__(256) batch_round_kernel(const BatchTickArgs T,
     __syncthreads();
     if (is_last) {
       __threadfence();
-      reduce_partials<L>(T.partials, R.first_item, R.num_items, d, smem, g_sm, F);
-      if (tid < 32) finalize_round<L>(R.args, E, F, g_sm, msg);
+      reduce_partials<L, K, DMAX + 1>(T.partials, R.first_item, R.num_items, d, smem, g_sm, F);
+      if (tid < 32) finalize_round<L, K>(R.args, E, F, g_sm, msg);
       if (tid == 0) {
         __threadfence();
         *R.args.st.counter = 0;

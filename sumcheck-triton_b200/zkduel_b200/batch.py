@@ -94,15 +94,35 @@ class BatchProver:
         self.launch()
         self.wait()
 
-    def tick_times(self) -> list[list[float]]:
+    def tick_times(self) -> list[dict]:
+        """Per (field group, degree class): the proof indices and each tick's start, end and
+        duration (ms from the start of its group's last run; groups' origins differ)."""
         out = []
         lib = _lib.load()
         for g in self.groups:
             cnt = ctypes.c_int(0)
-            _lib.check(lib.sc_batch_tick_times(g.handle, None, 0, ctypes.byref(cnt)), "sc_batch_tick_times")
-            buf = (ctypes.c_float * max(1, cnt.value))()
-            _lib.check(lib.sc_batch_tick_times(g.handle, buf, cnt.value, ctypes.byref(cnt)), "sc_batch_tick_times")
-            out.append(list(buf)[: cnt.value])
+            _lib.check(lib.sc_batch_classes(g.handle, None, None, 0, ctypes.byref(cnt)), "sc_batch_classes")
+            ncls = cnt.value
+            dcls = (ctypes.c_int32 * max(1, ncls))()
+            ticks = (ctypes.c_int32 * max(1, ncls))()
+            _lib.check(lib.sc_batch_classes(g.handle, dcls, ticks, ncls, ctypes.byref(cnt)), "sc_batch_classes")
+            _lib.check(lib.sc_batch_tick_times(g.handle, None, None, 0, ctypes.byref(cnt)), "sc_batch_tick_times")
+            t0 = (ctypes.c_float * max(1, cnt.value))()
+            t1 = (ctypes.c_float * max(1, cnt.value))()
+            _lib.check(lib.sc_batch_tick_times(g.handle, t0, t1, cnt.value, ctypes.byref(cnt)), "sc_batch_tick_times")
+            starts, ends = list(t0)[: cnt.value], list(t1)[: cnt.value]
+            pos = 0
+            for c in range(ncls):
+                _lib.check(lib.sc_batch_class_proofs(g.handle, c, None, 0, ctypes.byref(cnt)), "sc_batch_class_proofs")
+                idx = (ctypes.c_int32 * max(1, cnt.value))()
+                _lib.check(lib.sc_batch_class_proofs(g.handle, c, idx, cnt.value, ctypes.byref(cnt)),
+                           "sc_batch_class_proofs")
+                sl = slice(pos, pos + ticks[c])
+                out.append({"limbs": g.spec.limbs, "degree_class": int(dcls[c]),
+                            "proofs": [g.indices[k] for k in list(idx)[: cnt.value]],
+                            "start": starts[sl], "end": ends[sl],
+                            "ms": [b - a for a, b in zip(starts[sl], ends[sl])]})
+                pos += ticks[c]
         return out
 
     def result(self, i: int) -> Proof:

@@ -77,9 +77,12 @@ def test_stream_batch_replays_identically():
     for i in (0, 7, 23, 47):
         s = specs[i]
         _same(first[i], api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
-    times = bp.tick_times()
-    assert len(times) == 2 and all(len(t) == max(specs[i].num_vars for i in g.indices) for t, g in zip(times, bp.groups))
-    assert all(x > 0 for t in times for x in t)
+    classes = bp.tick_times()
+    assert sorted(i for c in classes for i in c["proofs"]) == list(range(len(specs)))
+    for c in classes:
+        assert len(c["ms"]) == max(specs[i].num_vars for i in c["proofs"])
+        assert all(x > 0 for x in c["ms"])
+        assert all(specs[i].degree <= c["degree_class"] for i in c["proofs"])
 
 
 def test_fixed_mode_and_rejects_explicit():
