@@ -17,7 +17,13 @@ Prints one JSON line (rank 0):
              speed-up);
   roofline   the dominant round kernel (by time) against its bound: integer multiply-adds
              against the measured IMAD rate (256-bit) or bytes against measured HBM GB/s;
-  cpu_baseline  the C oracle (all host threads) on a bounded sample of the same stream.
+  cpu_baseline  the C oracle (all host threads) on a bounded sample of the same stream;
+  served     the served stream (zkduel_b200.streams.served_stream: 20,000 requests over
+             2^127 - 1, num_vars log-uniform 12..24, degree 3-7 over up to 8 tables, Poisson
+             arrivals at the rate that keeps the FIFO-plain server 80% busy, measured first)
+             replayed in real time through the continuous-batching server and through the
+             FIFO-plain server, 150 GB admission budget: proofs/s and p50/p90/p99 latency
+             (host-observed completion minus submission) for both.
 --impl reference times that CPU port alone on the same workload (the reference's own
 prover is Python-only and cannot run here; the port restates it and is pinned against it).
 """
@@ -42,6 +48,9 @@ METRIC = "sumcheck_proofs_per_s_mixed_stream"
 WORKLOAD = "batched_512"
 STREAM_COUNT = 512
 PEAKS = ROOT / "MEASURED_PEAKS.json"
+SERVED_COUNT = 20000
+SERVED_LOAD = 0.8
+SERVED_BUDGET = 150 * 10**9
 
 
 def parse():
@@ -53,6 +62,8 @@ def parse():
     ap.add_argument("--path", choices=["batched", "plain"], default="batched")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--served", type=int, default=SERVED_COUNT,
+                    help="requests in the served stream (0: skip the served measurement)")
     ap.add_argument("--case", default=None,
                     help="profile mode: prove one plain config (plain_p32|plain_goldilocks|plain_bls) twice and exit")
     ap.add_argument("--case-vars", type=int, default=None, help="num_vars for --case (default: the config's)")
@@ -202,6 +213,17 @@ def max_over_ranks(x: float, world: int) -> float:
 
     t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -457,6 +479,10 @@ def main() -> int:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
                                 "sample": f"{done} proofs (every 16th of the 512-proof stream), {spent:.1f} s"}
+    if args.served > 0:
+        del batcher, steps_fn, work
+        torch.cuda.empty_cache()
+        line["served"] = served_measure(args, device, rank, world)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -464,6 +490,60 @@ def main() -> int:
 
         dist.destroy_process_group()
     return 0
+
+
+def served_measure(args, device, rank: int, world: int) -> dict:
+    """The served stream through both server policies (one server per rank, own stream)."""
+    import torch
+
+    from zkduel_b200 import api
+    from zkduel_b200.fields import get_field
+    from zkduel_b200.serve import ProofServer, replay
+    from zkduel_b200.streams import served_stream
+
+    spec = get_field(128)
+    dev = device.index
+    reserve = 32 << 30
+    # E[plain service time]: a burst through the FIFO-plain server (busy time / requests)
+    cal = served_stream(300, rate_per_s=1e9, seed=1000 + rank)
+    with ProofServer(spec, policy="fifo_plain", budget_bytes=SERVED_BUDGET, device=dev) as srv:
+        srv.reserve(reserve)
+        replay(srv, cal[:30])
+        b0 = srv.stats()["busy_s"]
+        replay(srv, cal)
+        service_s = (srv.stats()["busy_s"] - b0) / len(cal)
+    rate = SERVED_LOAD / service_s
+    reqs = served_stream(args.served, rate_per_s=rate, seed=1 + rank)
+    check = {0, len(reqs) // 2, len(reqs) - 1}
+    out = {"requests_per_gpu": len(reqs), "field": "2^127-1 (4 limbs)", "load": SERVED_LOAD,
+           "arrival_rate_per_s": rate, "plain_service_ms": service_s * 1e3, "budget_bytes": SERVED_BUDGET,
+           "latency": "host-observed completion minus submission"}
+    for pol in ("continuous", "fifo_plain"):
+        with ProofServer(spec, policy=pol, budget_bytes=SERVED_BUDGET, device=dev) as srv:
+            srv.reserve(reserve)
+            replay(srv, served_stream(50, rate_per_s=rate, seed=99))
+            rep, kept = replay(srv, reqs, keep_results=check)
+        summ = rep.summary()
+        # bit-exactness on a sample: the served result equals the proof alone
+        for i in sorted(check):
+            s = reqs[i].spec
+            t = api.generate_tables(spec, s.num_tables, s.num_vars, [0] * s.num_tables, s.seed, device)
+            alone = api.prove_device(t, s.expression, spec, s.num_vars, "sha3")
+            got = kept[i]
+            assert (got.checksum == alone.checksum and (got.round_polys_mont == alone.round_polys_mont).all()
+                    and (got.finals_mont == alone.finals_mont).all()), f"served request {i} differs from its proof alone"
+            del t
+        summ["bit_exact_sample"] = sorted(check)
+        if world > 1:
+            summ["proofs_per_s"] = sum_over_ranks(summ["proofs_per_s"], world)
+            for k in ("p50_ms", "p90_ms", "p99_ms", "mean_ms"):
+                summ[k] = max_over_ranks(summ[k], world)
+        out[pol] = summ
+    c, f = out["continuous"], out["fifo_plain"]
+    out["p50_speedup_vs_fifo"] = f["p50_ms"] / c["p50_ms"]
+    out["p99_speedup_vs_fifo"] = f["p99_ms"] / c["p99_ms"]
+    torch.cuda.synchronize(device)
+    return out
 
 
 def e2e_measure(work: Workload, args, device, batcher=None) -> dict:

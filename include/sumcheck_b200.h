@@ -35,6 +35,8 @@ extern "C" {
 #define SC_ERR_UNSUPPORTED 4    /* outside the compiled limits (degree, tables, terms)  */
 #define SC_ERR_DEVICE 5         /* the device reported an error status                  */
 #define SC_ERR_NOMEM 6          /* device or host allocation failed                     */
+#define SC_ERR_TIMEOUT 7        /* a bounded wait ran out (sc_server_wait / _drain)     */
+#define SC_ERR_PENDING 8        /* the request has not completed yet                    */
 
 #define SC_CHALLENGE_SHA3 0     /* r_j = SHA3 transcript rule (field_sumcheck.cu:857-907) */
 #define SC_CHALLENGE_FIXED 1    /* r_j = 1 (field_sumcheck.cu:1058)                       */
@@ -202,6 +204,82 @@ int sc_batch_class_proofs(sc_batch* batch, int cls, int32_t* out_indices, int ca
 int sc_batch_tick_times(sc_batch* batch, float* out_start_ms, float* out_end_ms, int capacity,
                         int* count);
 int sc_batch_destroy(sc_batch* batch);
+
+/* ---- Served proving -------------------------------------------------------------------
+ * Replaces: nothing in the reference runs more than one proof at a time; its callers loop
+ * over proofs (cuda/src/field_sumcheck.cu:1178-1336, src/zkduel/api.py:26-64).
+ *
+ * A server owns one GPU stream, a device memory pool and a worker thread. A request is the
+ * call (expression, num_rounds, table kinds, seed, challenge mode): its tables are
+ * generated on the device from the seed when it is admitted and stay resident, with its
+ * fold buffers and transcript state, until it completes. Requests are admitted in arrival
+ * order while the sum of admitted footprints (tables + fold buffers + partials + state)
+ * stays within hbm_budget_bytes and fewer than max_inflight are in flight.
+ *
+ * SC_SERVE_CONTINUOUS: continuous batching. Every tick is one launch per degree class of
+ *   the batched round kernel over (request, tile) items of the in-flight requests: each
+ *   request whose current round has at most one wave of tiles left runs all of them, and
+ *   the larger rounds share `chunk_items` tiles per tick, oldest request first (it gets one
+ *   wave at least), advancing over several ticks. Requests join at the next tick after
+ *   admission and leave after their last round, so arrivals overlap on the device with
+ *   work already running.
+ * SC_SERVE_FIFO_PLAIN: the baseline; one request at a time, in arrival order, each proved
+ *   by the plain path (sc_prove) after its tables are generated.
+ * Results are bit-identical to sc_prove on sc_tables_generate's tables for the same seed.
+ * Times are seconds on the host's steady clock since sc_server_create. */
+typedef struct sc_server sc_server;
+
+#define SC_SERVE_CONTINUOUS 0
+#define SC_SERVE_FIFO_PLAIN 1
+
+typedef struct sc_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t ticks;              /* launches groups issued (continuous policy) */
+  uint64_t items;              /* (request, tile) items issued */
+  uint64_t peak_inflight;      /* most requests admitted at once */
+  uint64_t peak_footprint;     /* most bytes admitted at once */
+  uint64_t budget;             /* hbm_budget_bytes */
+  double busy_s;               /* host-observed time with at least one request in flight */
+  double alloc_s;              /* worker time in pool allocations (admission) */
+  double wait_s;               /* worker time blocked on the GPU (tick ring full / draining) */
+  double build_s;              /* worker time composing and issuing ticks */
+} sc_server_stats;
+
+/* threads: 0 = default; pairs_per_thread: 0 = 4 (a tile is threads x pairs_per_thread
+ * pairs); chunk_items: tiles per tick for the larger rounds, 0 = two waves of the grid. */
+int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm_budget_bytes,
+                     int max_inflight, int max_tables, int threads, int pairs_per_thread,
+                     int chunk_items, sc_server** out);
+/* Maps `bytes` of device memory into the server's pool ahead of time (allocates and frees
+ * them; the pool keeps freed memory), so admissions up to that much do not grow the pool
+ * while requests run. Synchronous. */
+int sc_server_reserve(sc_server* server, uint64_t bytes);
+/* Footprint a request would be admitted with; SC_ERR_UNSUPPORTED beyond the budget. */
+int sc_server_footprint(const sc_server* server, const sc_expr* expr, int num_rounds,
+                        uint64_t* out_bytes);
+/* Queues a request (thread-safe; returns at once). table_kinds: expr's num_vars entries
+ * of SC_TABLE_*. The expression is copied. */
+int sc_server_submit(sc_server* server, const sc_expr* expr, int num_rounds,
+                     const int32_t* table_kinds, uint64_t seed, int challenge_mode,
+                     uint64_t* out_id);
+/* Waits until request `id` completed (SC_OK), failed (its error code), or timeout_ms
+ * passed (SC_ERR_TIMEOUT). timeout_ms < 0 waits without limit. */
+int sc_server_wait(sc_server* server, uint64_t id, int timeout_ms);
+/* Waits until every submitted request completed or failed. */
+int sc_server_drain(sc_server* server, int timeout_ms);
+/* Outputs of a completed request, laid out as sc_prove's; SC_ERR_PENDING before that. */
+int sc_server_result(sc_server* server, uint64_t id, uint32_t* out_round_polys,
+                     uint32_t* out_challenges, uint32_t* out_finals, uint32_t* out_claim0,
+                     uint64_t* out_checksum);
+/* Submit, admission and completion times of a request (completion: when the server saw
+ * its last round and result copy finish). */
+int sc_server_times(sc_server* server, uint64_t id, double* out_submit_s, double* out_admit_s,
+                    double* out_done_s);
+/* Forgets a completed request (its result is no longer readable). */
+int sc_server_release(sc_server* server, uint64_t id);
+int sc_server_stats_get(sc_server* server, sc_server_stats* out);
+/* Stops accepting requests, finishes the queued ones, joins the worker, frees everything. */
+int sc_server_destroy(sc_server* server);
 
 #ifdef __cplusplus
 }

@@ -17,8 +17,10 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "zkduel_b200" / "libsumcheck_b200.so"
+OBJ = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
+SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "serve.cu"]
 
 
 def _stale(target: Path, deps) -> bool:
@@ -33,13 +35,25 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     hdr = CSRC / "field_ptx.cuh"
     if _stale(hdr, [gen]):
         subprocess.check_call([sys.executable, str(gen)])
-    sources = [CSRC / "capi.cu", CSRC / "batch.cu", CSRC / "noalloc.cu"]
-    deps = sources + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "sumcheck_b200.h"]
-    if not force and not _stale(LIB, deps):
+    sources = [CSRC / s for s in SOURCES]
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "sumcheck_b200.h"]
+    if not force and not _stale(LIB, sources + headers):
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), *map(str, sources), "-o", str(LIB)]
-    subprocess.check_call(cmd)
+    OBJ.mkdir(exist_ok=True)
+    # one nvcc per translation unit, in parallel; then one link
+    procs = []
+    for src in sources:
+        obj = OBJ / (src.stem + ".o")
+        if not force and not _stale(obj, [src] + headers):
+            continue
+        cmd = [nvcc, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-c", str(src), "-o", str(obj)]
+        procs.append((src, subprocess.Popen(cmd)))
+    failed = [str(src) for src, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, f"nvcc {' '.join(failed)}")
+    objs = [str(OBJ / (src.stem + ".o")) for src in sources]
+    subprocess.check_call([nvcc, *ARCH, "-shared", *objs, "-o", str(LIB)])
     return LIB
 
 

@@ -60,36 +60,62 @@ struct sc_batch {
 namespace {
 
 template <int L, int K, int D>
-struct BatchClassSetup {
-  static int run(sc_batch* B, BatchClass& C, int kmax) {
-    int threads = std::min(B->threads_req ? B->threads_req : kernel_threads(L), kernel_threads(L));
+struct KernelSetup {
+  static int run(int kmax, int threads_req, int sm_count, int* threads_out, int* grid_out, size_t* smem_out) {
+    int threads = std::min(threads_req ? threads_req : kernel_threads(L), kernel_threads(L));
     const int per_thread = round_smem_words_per_thread(kmax, L) * 4;
     while (threads > 32 && static_cast<size_t>(threads) * per_thread > static_cast<size_t>(kMaxDynSmem)) threads -= 32;
-    C.threads = threads;
-    C.smem = static_cast<size_t>(threads) * per_thread;
+    const size_t smem = static_cast<size_t>(threads) * per_thread;
     SC_CUDA(cudaFuncSetAttribute(batch_round_kernel<L, K, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
     int bps = 0;
-    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_round_kernel<L, K, D>, threads, C.smem));
-    if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "batch kernel does not fit on an SM (K=%d, L=%d)", kmax, L);
-    C.grid = bps * B->ctx->sm_count;
+    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_round_kernel<L, K, D>, threads, smem));
+    if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "batch kernel does not fit on an SM (tables=%d, L=%d)", kmax, L);
+    *threads_out = threads;
+    *grid_out = bps * sm_count;
+    *smem_out = smem;
     return SC_OK;
   }
 };
 
 template <int L, int K, int D>
-struct BatchTick {
-  static int run(sc_batch* B, const BatchClass& C, int t, const BatchTickArgs& T) {
+struct KernelLaunch {
+  static int run(const sc_field* field, unsigned grid, int threads, size_t smem, cudaStream_t stream,
+                 const BatchTickArgs& T) {
     FieldParams<L, K> F;
-    for (int l = 0; l < L; ++l) F.p[l] = B->field->hf.p[l];
-    F.np = B->field->hf.np;
-    const unsigned grid = static_cast<unsigned>(std::min(C.grid, std::max(1, T.num_items)));
-    SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t], C.stream, cudaEventRecordExternal));
-    batch_round_kernel<L, K, D><<<grid, C.threads, C.smem, C.stream>>>(T, F);
+    for (int l = 0; l < L; ++l) F.p[l] = field->hf.p[l];
+    F.np = field->hf.np;
+    batch_round_kernel<L, K, D><<<grid, threads, smem, stream>>>(T, F);
     SC_CUDA(cudaGetLastError());
-    SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t + 1], C.stream, cudaEventRecordExternal));
     return SC_OK;
   }
 };
+
+}  // namespace
+
+namespace sc_host {
+
+int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int sm_count, int* threads, int* grid,
+                       size_t* smem) {
+  return dispatch<KernelSetup>(L, K, dclass, kmax, threads_req, sm_count, threads, grid, smem);
+}
+
+int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
+                        cudaStream_t stream, const BatchTickArgs& T) {
+  return dispatch<KernelLaunch>(L, K, dclass, field, grid, threads, smem, stream, T);
+}
+
+}  // namespace sc_host
+
+namespace {
+
+int batch_tick(sc_batch* B, const BatchClass& C, int t, const BatchTickArgs& T) {
+  const unsigned grid = static_cast<unsigned>(std::min(C.grid, std::max(1, T.num_items)));
+  SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t], C.stream, cudaEventRecordExternal));
+  const int rc = batch_kernel_launch(B->L, B->kind, C.dclass, B->field, grid, C.threads, C.smem, C.stream, T);
+  if (rc) return rc;
+  SC_CUDA(cudaEventRecordWithFlags(C.tick_events[2 * t + 1], C.stream, cudaEventRecordExternal));
+  return SC_OK;
+}
 
 template <int L>
 int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const* tables) {
@@ -114,7 +140,8 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
         C.max_rounds = std::max(C.max_rounds, B->n[p]);
       }
     if (C.proofs.empty()) continue;
-    if ((rc = dispatch<BatchClassSetup>(L, B->kind, dc, B, C, kmax))) return rc;
+    if ((rc = batch_kernel_setup(L, B->kind, dc, kmax, B->threads_req, ctx->sm_count, &C.threads, &C.grid, &C.smem)))
+      return rc;
     B->classes.push_back(std::move(C));
   }
   // per-proof state and fold buffers (16-byte aligned carve-outs of two pools)
@@ -136,8 +163,11 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
   SC_CUDA(cudaMallocHost(&B->host_state, B->state_words * 4));
   uint32_t* st = static_cast<uint32_t*>(B->state.p);
   uint32_t* pool = static_cast<uint32_t*>(B->fold_pool.p);
+  if ((rc = ensure(ctx, B->exprs, ed.size() * sizeof(ExprDev)))) return rc;
+  const ExprDev* exprs_dev = static_cast<const ExprDev*>(B->exprs.p);
   // every class's ticks: rounds and items, in one array each (class and tick offsets)
   std::vector<BatchRound> rounds;
+  std::vector<size_t> partial_item;  // per round: index of its first partial slot
   std::vector<BatchItem> items;
   for (BatchClass& C : B->classes) {
     C.head0 = B->total_heads;
@@ -180,11 +210,14 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
         A.st.finals = s + o.finals;
         A.st.claim0 = s + o.claim0;
         A.st.claim = s + o.claim;
-        R.expr = p;
+        R.expr = exprs_dev + p;
         const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt;
         const uint64_t nitems = (A.pairs + tile - 1) / tile;
         R.first_item = static_cast<int>(items.size()) - C.tick_item0[t];  // tick-relative
         R.num_items = static_cast<int>(nitems);
+        R.item_base = 0;
+        R.round_items = static_cast<int>(nitems);
+        partial_item.push_back(items.size());
         const int ridx = static_cast<int>(rounds.size()) - C.tick_round0[t];
         for (uint64_t i = 0; i < nitems; ++i) {
           BatchItem I;
@@ -204,7 +237,8 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
   if ((rc = ensure(ctx, B->rounds, rounds.size() * sizeof(BatchRound)))) return rc;
   if ((rc = ensure(ctx, B->items, items.size() * sizeof(BatchItem)))) return rc;
   if ((rc = ensure(ctx, B->heads, static_cast<size_t>(std::max(1, B->total_heads)) * 4))) return rc;
-  if ((rc = ensure(ctx, B->exprs, ed.size() * sizeof(ExprDev)))) return rc;
+  for (size_t r = 0; r < rounds.size(); ++r)
+    rounds[r].partials = static_cast<uint32_t*>(B->partials.p) + partial_item[r] * kMaxPoints * L;
   SC_CUDA(cudaMemcpy(B->rounds.p, rounds.data(), rounds.size() * sizeof(BatchRound), cudaMemcpyHostToDevice));
   SC_CUDA(cudaMemcpy(B->items.p, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
   SC_CUDA(cudaMemcpy(B->exprs.p, ed.data(), ed.size() * sizeof(ExprDev), cudaMemcpyHostToDevice));
@@ -226,9 +260,7 @@ int batch_issue(sc_batch* B) {
       T.num_items = C.tick_items[t];
       T.pad = 0;
       T.head = static_cast<uint32_t*>(B->heads.p) + C.head0 + t;
-      T.exprs = static_cast<const ExprDev*>(B->exprs.p);
-      T.partials = static_cast<uint32_t*>(B->partials.p) + static_cast<size_t>(C.tick_item0[t]) * kMaxPoints * B->L;
-      const int rc = dispatch<BatchTick>(B->L, B->kind, C.dclass, B, C, t, T);
+      const int rc = batch_tick(B, C, t, T);
       if (rc) return rc;
     }
     SC_CUDA(cudaEventRecord(C.done, C.stream));

@@ -47,6 +47,14 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// The batched round kernel's launch shape and launch (instantiated once, in batch.cu):
+// threads per block, grid (resident blocks on every SM) and dynamic shared memory for
+// requests of up to kmax tables.
+int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int sm_count, int* threads, int* grid,
+                       size_t* smem);
+int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
+                        cudaStream_t stream, const BatchTickArgs& T);
+
 }  // namespace sc_host
 
 using sc_host::DevBuf;
@@ -302,5 +310,13 @@ inline StateOffsets state_offsets(int n, int K, int L) {
   o.total_words = o.claim + L;
   return o;
 }
+
+// The batched round kernel's launch shape and launch (instantiated once, in batch.cu):
+// threads per block, grid (resident blocks on every SM) and dynamic shared memory for
+// requests of up to kmax tables.
+int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int sm_count, int* threads, int* grid,
+                       size_t* smem);
+int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
+                        cudaStream_t stream, const BatchTickArgs& T);
 
 }  // namespace sc_host

@@ -480,19 +480,23 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
 
 // ------------------------------------------------------------------------------ batched
 //
-// Many independent proofs advance one round per "tick". A tick is one launch per (field,
-// degree class): a persistent kernel whose blocks pull (proof round, tile of pairs) items
-// from a device work queue (an atomic counter over the tick's item list). Every item leaves
-// one partial; the block that finishes the last item of a proof's round (per-proof atomic
-// ticket) reduces that proof's partials and finalises its round -- SHA3 challenge included
-// -- while the other blocks go on with other proofs' items.
+// Many independent proofs advance together, one launch per "tick" and degree class: a
+// persistent kernel whose blocks pull (proof round, tile of pairs) items from a device work
+// queue (an atomic counter over the tick's item list). Every item leaves one partial in its
+// round's partial slots; the block that finishes the last item of a proof's round (per-proof
+// atomic ticket) reduces that round's partials and finalises it -- SHA3 challenge included --
+// while the other blocks go on with other proofs' items. A round's items may be spread over
+// several ticks (the served prover slices large rounds): the ticket counts to the round's
+// item total, whichever tick its last item runs in.
 
 struct BatchRound {
-  RoundArgs args;      // this proof's round (src/dst/len/pairs/round/fold/mode/flags/fc/state)
-  int32_t expr;        // index into the batch's expression table
-  int32_t first_item;  // this round's items: [first_item, first_item + num_items) of the tick
+  RoundArgs args;        // this proof's round (src/dst/len/pairs/round/fold/mode/flags/fc/state)
+  const ExprDev* expr;   // this proof's expression
+  uint32_t* partials;    // the round's partial slots: [round_items][kMaxPoints][L]
+  int32_t first_item;    // this tick's items of the round: [first_item, first_item + num_items)
   int32_t num_items;
-  int32_t pad;
+  int32_t item_base;     // round-relative index of this tick's first item of the round
+  int32_t round_items;   // items of the whole round, over all ticks
 };
 
 struct BatchItem {
@@ -508,8 +512,6 @@ struct BatchTickArgs {
   int32_t num_items;
   int32_t pad;
   uint32_t* head;      // queue counter of this tick (zero before the launch)
-  const ExprDev* exprs;
-  uint32_t* partials;  // [num_items][kMaxPoints][L], indexed by item
 };
 
 template <int L, int K, int DMAX>
@@ -520,10 +522,11 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
   __shared__ __align__(16) uint8_t msg[3 * 136];
   __shared__ __align__(16) ExprDev E;
   __shared__ __align__(16) BatchRound R;
-  __shared__ int item_sm, is_last, cur_expr;
+  __shared__ const ExprDev* cur_expr;
+  __shared__ int item_sm, is_last;
 
   const int tid = threadIdx.x, nthr = blockDim.x;
-  if (tid == 0) cur_expr = -1;
+  if (tid == 0) cur_expr = nullptr;
   for (;;) {
     __syncthreads();
     if (tid == 0) item_sm = static_cast<int>(atomicAdd(T.head, 1u));
@@ -534,7 +537,7 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
     if (tid == 0) R = T.rounds[I.round];
     __syncthreads();
     if (R.expr != cur_expr) {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(T.exprs + R.expr);
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(R.expr);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&E);
       for (int i = tid; i < static_cast<int>(sizeof(ExprDev) / 4); i += nthr) dst[i] = src[i];
       __syncthreads();
@@ -552,14 +555,15 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
                               I.start + tid, I.start + I.count, nthr, R.args.skip1 != 0, acc, F);
     __syncthreads();
     block_reduce<L, K, DMAX + 1>(acc, d, smem, g_sm, F);
-    for (int i = tid; i < (d + 1) * L; i += nthr) T.partials[static_cast<uint64_t>(it) * kMaxPoints * L + i] = g_sm[i];
+    uint32_t* slot = R.partials + static_cast<uint64_t>(R.item_base + (it - R.first_item)) * kMaxPoints * L;
+    for (int i = tid; i < (d + 1) * L; i += nthr) slot[i] = g_sm[i];
     __threadfence();
     __syncthreads();
-    if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.num_items - 1));
+    if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.round_items - 1));
     __syncthreads();
     if (is_last) {
       __threadfence();
-      reduce_partials<L, K, DMAX + 1>(T.partials, R.first_item, R.num_items, d, smem, g_sm, F);
+      reduce_partials<L, K, DMAX + 1>(R.partials, 0, R.round_items, d, smem, g_sm, F);
       if (tid < 32) finalize_round<L, K>(R.args, E, F, g_sm, msg);
       if (tid == 0) {
         __threadfence();

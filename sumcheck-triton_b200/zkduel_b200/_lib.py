@@ -22,6 +22,12 @@ SC_ERR_CUDA = 3
 SC_ERR_UNSUPPORTED = 4
 SC_ERR_DEVICE = 5
 SC_ERR_NOMEM = 6
+SC_ERR_TIMEOUT = 7
+SC_ERR_PENDING = 8
+
+SC_SERVE_CONTINUOUS = 0
+SC_SERVE_FIFO_PLAIN = 1
+SERVE_POLICIES = {"continuous": SC_SERVE_CONTINUOUS, "fifo_plain": SC_SERVE_FIFO_PLAIN}
 
 SC_CHALLENGE_SHA3 = 0
 SC_CHALLENGE_FIXED = 1
@@ -34,6 +40,18 @@ SC_TABLE_ARITH = 2
 
 U32P = POINTER(c_uint32)
 U64P = POINTER(c_uint64)
+F64P = POINTER(c_double)
+
+
+class ServerStats(ctypes.Structure):
+    """sc_server_stats."""
+
+    _fields_ = [
+        ("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("ticks", c_uint64),
+        ("items", c_uint64), ("peak_inflight", c_uint64), ("peak_footprint", c_uint64), ("budget", c_uint64),
+        ("busy_s", c_double), ("alloc_s", c_double), ("wait_s", c_double), ("build_s", c_double),
+    ]
+
 
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
@@ -74,6 +92,19 @@ SIGNATURES = {
     "sc_batch_class_proofs": (c_int, [c_void_p, c_int, POINTER(c_int32), c_int, POINTER(c_int)]),
     "sc_batch_destroy": (c_int, [c_void_p]),
     "sc_calibrate_imad": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_server_create": (
+        c_int, [c_int, c_void_p, c_int, c_uint64, c_int, c_int, c_int, c_int, c_int, POINTER(c_void_p)],
+    ),
+    "sc_server_footprint": (c_int, [c_void_p, c_void_p, c_int, U64P]),
+    "sc_server_reserve": (c_int, [c_void_p, c_uint64]),
+    "sc_server_submit": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_int32), c_uint64, c_int, U64P]),
+    "sc_server_wait": (c_int, [c_void_p, c_uint64, c_int]),
+    "sc_server_drain": (c_int, [c_void_p, c_int]),
+    "sc_server_result": (c_int, [c_void_p, c_uint64, U32P, U32P, U32P, U32P, U64P]),
+    "sc_server_times": (c_int, [c_void_p, c_uint64, F64P, F64P, F64P]),
+    "sc_server_release": (c_int, [c_void_p, c_uint64]),
+    "sc_server_stats_get": (c_int, [c_void_p, POINTER(ServerStats)]),
+    "sc_server_destroy": (c_int, [c_void_p]),
     "sc_prove": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, U32P, U32P, U32P, U32P, U32P, U64P],
@@ -121,6 +152,8 @@ def check(rc: int, what: str) -> None:
         raise ValueError(msg)
     if rc == SC_ERR_NOMEM:
         raise MemoryError(msg)
+    if rc == SC_ERR_TIMEOUT:
+        raise TimeoutError(msg)
     raise SumcheckError(msg)
 
 
