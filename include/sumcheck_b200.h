@@ -216,7 +216,10 @@ int sc_batch_destroy(sc_batch* batch);
  * order while the sum of admitted footprints (tables + fold buffers + partials + state)
  * stays within hbm_budget_bytes and fewer than max_inflight are in flight.
  *
- * SC_SERVE_CONTINUOUS: continuous batching. Every tick is one launch per degree class of
+ * SC_SERVE_CONTINUOUS: continuous batching. A request whose round 0 is larger than one wave
+ *   of the GPU runs whole on a low-priority stream (one launch per round, one block per
+ *   tile); the others are batched in ticks on high-priority streams, so they overtake the
+ *   large proofs on the device. Every tick is one launch per degree class of
  *   the batched round kernel over (request, tile) items of the in-flight requests: each
  *   request whose current round has at most one wave of tiles left runs all of them, and
  *   the larger rounds share `chunk_items` tiles per tick, oldest request first (it gets one

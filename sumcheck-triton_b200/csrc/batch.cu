@@ -260,6 +260,7 @@ int batch_issue(sc_batch* B) {
       T.num_items = C.tick_items[t];
       T.pad = 0;
       T.head = static_cast<uint32_t*>(B->heads.p) + C.head0 + t;
+      T.tile = 0;
       const int rc = batch_tick(B, C, t, T);
       if (rc) return rc;
     }

@@ -35,18 +35,32 @@ struct ProveRun {
     const StateOffsets so = state_offsets(n, K_, L);
     if ((rc = ensure(ctx, ctx->state, so.total_words * 4))) return rc;
 
+    ExprDev E;
+    build_expr_dev<L>(*ex, *f, E);
+    // the kernel: a compile-time shape when the expression has one, else the generic evaluator
+    using Kern = void (*)(const RoundArgs, const ExprDev, const FieldParams<L, K>);
+    Kern kern = round_kernel<L, K, DMAX>;
+    int shape = kShapeGeneric;
+    if constexpr (DMAX == 4) {
+      if (E.shape == kShapeZerocheck) kern = round_kernel<L, K, 4, kShapeZerocheck>;
+      if (E.shape == kShapeAbcg) kern = round_kernel<L, K, 4, kShapeAbcg>;
+      shape = E.shape;
+    }
     int threads = kernel_threads(L);
-    const int per_thread = round_smem_words_per_thread(K_, L) * 4;
-    while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
-    const size_t smem = static_cast<size_t>(threads) * per_thread;
+    size_t smem;
+    if (shape == kShapeGeneric) {
+      const int per_thread = round_smem_words_per_thread(K_, L) * 4;
+      while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
+      smem = static_cast<size_t>(threads) * per_thread;
+    } else {
+      smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
+    }
     int blocks_per_sm = 0;
-    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, round_kernel<L, K, DMAX>, threads, smem));
+    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, threads, smem));
     if (blocks_per_sm < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", K_, L);
     const uint64_t grid_max = static_cast<uint64_t>(blocks_per_sm) * ctx->sm_count;
     if ((rc = ensure(ctx, ctx->partials, grid_max * kMaxPoints * L * 4))) return rc;
 
-    ExprDev E;
-    build_expr_dev<L>(*ex, *f, E);
     FieldParams<L, K> F;
     for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
     F.np = f->hf.np;
@@ -93,7 +107,7 @@ struct ProveRun {
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
       cudaEvent_t ev;
       if ((rc = timing_begin(ctx, &ev))) return rc;
-      round_kernel<L, K, DMAX><<<grid, threads, smem, ctx->stream>>>(A, E, F);
+      kern<<<grid, threads, smem, ctx->stream>>>(A, E, F);
       SC_CUDA(cudaGetLastError());
       if ((rc = timing_end(ctx))) return rc;
     }

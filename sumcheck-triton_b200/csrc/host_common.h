@@ -240,9 +240,89 @@ inline bool extrapolate_term(int len, int d, int L, int K) {
   return extrap < direct;
 }
 
+// Matches the expression against the compile-time shapes (prover.cuh: Shape). Returns the
+// shape (kShapeGeneric when none matches) and fills role[] with the table of every role.
+// Coefficients must be exactly +1 (and -1 for the zerocheck's S4 X3 term); every table used
+// once per term, every role a different table.
+inline int match_shape(const sc_expr& ex, uint8_t* role) {
+  if (!ex.coeff_limbs.empty() || ex.degree != 4) return kShapeGeneric;
+  const int T = ex.num_terms;
+  std::vector<std::vector<int>> terms(T);
+  for (int i = 0; i < T; ++i) {
+    terms[i].assign(ex.flat.begin() + ex.offs[i], ex.flat.begin() + ex.offs[i] + ex.lens[i]);
+    std::vector<int> u = terms[i];
+    std::sort(u.begin(), u.end());
+    if (std::adjacent_find(u.begin(), u.end()) != u.end()) return kShapeGeneric;  // repeated factor
+  }
+  auto has = [](const std::vector<int>& v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); };
+  // the table common to every term
+  int common = -1;
+  for (int k = 0; k < ex.num_vars && common < 0; ++k) {
+    bool all = true;
+    for (int i = 0; i < T && all; ++i) all = has(terms[i], k);
+    if (all) common = k;
+  }
+  if (common < 0) return kShapeGeneric;
+  std::vector<std::vector<int>> rest(T);
+  for (int i = 0; i < T; ++i)
+    for (int x : terms[i])
+      if (x != common) rest[i].push_back(x);
+  auto distinct_all = [&](const std::vector<int>& r) {
+    if (static_cast<int>(r.size()) != ex.num_vars) return false;
+    std::vector<int> u = r;
+    std::sort(u.begin(), u.end());
+    for (int k = 0; k < ex.num_vars; ++k)
+      if (u[k] != k) return false;
+    return true;
+  };
+  if (T == 2 && ex.num_vars == 6 && ex.coeffs[0] == 1 && ex.coeffs[1] == 1) {
+    const int i3 = rest[0].size() == 3 ? 0 : 1;
+    const std::vector<int>& a = rest[i3];
+    const std::vector<int>& b = rest[1 - i3];
+    if (a.size() != 3 || b.size() != 2) return kShapeGeneric;
+    const std::vector<int> r = {a[0], a[1], a[2], common, b[0], b[1]};
+    if (!distinct_all(r)) return kShapeGeneric;
+    for (int i = 0; i < 6; ++i) role[i] = static_cast<uint8_t>(r[i]);
+    return kShapeAbcg;
+  }
+  if (T == 5 && ex.num_vars == 9) {
+    int m = -1, c1 = -1, neg = -1;
+    std::vector<int> pos2;
+    for (int i = 0; i < T; ++i) {
+      const size_t n = rest[i].size();
+      const int64_t c = ex.coeffs[i];
+      if (n == 3 && c == 1 && m < 0) m = i;
+      else if (n == 1 && c == 1 && c1 < 0) c1 = i;
+      else if (n == 2 && c == -1 && neg < 0) neg = i;
+      else if (n == 2 && c == 1) pos2.push_back(i);
+      else return kShapeGeneric;
+    }
+    if (m < 0 || c1 < 0 || neg < 0 || pos2.size() != 2) return kShapeGeneric;
+    const std::vector<int>& M = rest[m];
+    int x[2], sel[2];
+    for (int j = 0; j < 2; ++j) {
+      const std::vector<int>& P = rest[pos2[j]];
+      const bool in0 = has(M, P[0]), in1 = has(M, P[1]);
+      if (in0 == in1) return kShapeGeneric;  // exactly one factor shared with the degree-3 term
+      x[j] = in0 ? P[0] : P[1];
+      sel[j] = in0 ? P[1] : P[0];
+    }
+    if (x[0] == x[1]) return kShapeGeneric;
+    int mr = -1;
+    for (int v : M)
+      if (v != x[0] && v != x[1]) mr = v;
+    const std::vector<int> r = {sel[0], x[0], common, sel[1], x[1], mr, rest[neg][0], rest[neg][1], rest[c1][0]};
+    if (mr < 0 || !distinct_all(r)) return kShapeGeneric;
+    for (int i = 0; i < 9; ++i) role[i] = static_cast<uint8_t>(r[i]);
+    return kShapeZerocheck;
+  }
+  return kShapeGeneric;
+}
+
 template <int L>
 inline void build_expr_dev(const sc_expr& ex, const sc_field& f, ExprDev& E) {
   std::memset(&E, 0, sizeof(E));
+  E.shape = match_shape(ex, E.role);
   E.num_vars = ex.num_vars;
   E.num_terms = ex.num_terms;
   E.degree = ex.degree;

@@ -25,6 +25,7 @@
 // points; the host picks the smallest class >= the expression's degree).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "field.cuh"
 #include "keccak.cuh"
@@ -69,7 +70,22 @@ struct ExprDev {
   uint8_t term_extrap[kMaxTerms];   // 1: evaluate points 0..len only, extrapolate the rest
   int32_t coeff_small[kMaxTerms];
   uint32_t coeff_mont[kMaxTerms][kMaxLimbs];
+  int32_t shape;                    // Shape the host matched (kShapeGeneric: none)
+  uint8_t role[16];                 // shape kernels: table index of each role
 };
+
+// Expression shapes with a compile-time evaluator (the host matches the term structure and
+// maps tables to roles; any table order and any order of the symmetric factors matches):
+//   kShapeZerocheck  F (X1 S1 + X2 S2 + X1 X2 M - X3 S4 + S5)   roles S1 X1 F S2 X2 M S4 X3 S5
+//                    evaluated as F (X1 (S1 + M X2) + S2 X2 - S4 X3 + S5): 5 products a point
+//                    (the vanilla zerocheck gate, src/zkduel/workloads.py:37-43)
+//   kShapeAbcg       G (A B C + D E)                              roles A B C G D E
+//                    4 products a point (poly_abcg_plus_deg, workloads.py:32)
+enum Shape : int32_t { kShapeGeneric = 0, kShapeZerocheck = 1, kShapeAbcg = 2 };
+
+__host__ __device__ constexpr int shape_tables(int shape) {
+  return shape == kShapeZerocheck ? 9 : (shape == kShapeAbcg ? 6 : 0);
+}
 
 // Per-proof device state, all Montgomery limbs (written by the finalisation).
 struct ProofState {
@@ -230,17 +246,41 @@ __device__ __forceinline__ void eval_pair(const ExprDev& E, const uint32_t* sv, 
   }
 }
 
+template <int L, int K>
+__device__ __forceinline__ Fe<L> shape_value(const Fe<L> (&v)[9], const FieldParams<L, K>& F,
+                                             std::integral_constant<int, kShapeZerocheck>) {
+  const Fe<L> u = fe_add(v[0], fe_mul(v[5], v[4], F), F);  // S1 + M X2
+  Fe<L> s = fe_mul(v[1], u, F);                            // X1 (S1 + M X2)
+  s = fe_add(s, fe_mul(v[3], v[4], F), F);                 // + S2 X2
+  s = fe_sub(s, fe_mul(v[6], v[7], F), F);                 // - S4 X3
+  s = fe_add(s, v[8], F);                                  // + S5
+  return fe_mul(v[2], s, F);                               // F (...)
+}
+
+template <int L, int K>
+__device__ __forceinline__ Fe<L> shape_value(const Fe<L> (&v)[6], const FieldParams<L, K>& F,
+                                             std::integral_constant<int, kShapeAbcg>) {
+  const Fe<L> s = fe_add(fe_mul(fe_mul(v[0], v[1], F), v[2], F), fe_mul(v[4], v[5], F), F);
+  return fe_mul(v[3], s, F);
+}
+
 // Folds (if fold) and evaluates pairs q = first, first + stride, ... < last, adding the
-// point sums into acc. sv / sd: this block's [K][L][nthr] shared arrays.
-template <int L, int K, int DMAX>
+// point sums into acc. Generic: every table's value and difference go to this block's
+// [K][L][nthr] shared arrays sv / sd for eval_pair. Shape kernels keep them in registers
+// (tables read in role order) and evaluate the shape's compile-time formula at each point.
+template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>
 __device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst, uint64_t src_len, bool fold,
                                               const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
                                               uint64_t first, uint64_t last, uint64_t stride, bool skip1,
                                               Fe<L> (&acc)[DMAX + 1], const FieldParams<L, K>& F) {
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int nv = E.num_vars;
+  constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
+  const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
   for (uint64_t q = first; q < last; q += stride) {
-    for (int k = 0; k < nv; ++k) {
+    Fe<L> sh_v[NR], sh_d[NR];
+#pragma unroll (SHAPE == kShapeGeneric ? 1 : NR)
+    for (int i = 0; i < nv; ++i) {
+      const int k = SHAPE == kShapeGeneric ? i : E.role[i];
       Fe<L> e, o;
       if (fold) {
         Fe<L> x0, x1, x2, x3;
@@ -262,10 +302,35 @@ __device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst
           e.w[l] = v.x; o.w[l] = v.y;
         }
       }
-      sm_put<L>(sv, k, tid, nthr, e);
-      sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
+      if constexpr (SHAPE == kShapeGeneric) {
+        sm_put<L>(sv, k, tid, nthr, e);
+        sm_put<L>(sd, k, tid, nthr, fe_sub(o, e, F));
+      } else {
+        sh_v[i] = e;
+        sh_d[i] = o;  // o for now: the difference is formed below
+      }
     }
-    eval_pair<L, K, DMAX>(E, sv, sd, tid, nthr, skip1, acc, F);
+    if constexpr (SHAPE == kShapeGeneric) {
+      eval_pair<L, K, DMAX>(E, sv, sd, tid, nthr, skip1, acc, F);
+    } else {
+      // point 0: e; point 1: o (skipped when skip1); then v(t) = v(t - 1) + (o - e)
+      constexpr int D = 4;
+      static_assert(DMAX >= D, "shape kernels evaluate degree-4 shapes");
+      acc[0] = fe_add(acc[0], shape_value<L, K>(sh_v, F, std::integral_constant<int, SHAPE>{}), F);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const Fe<L> o = sh_d[r];
+        sh_d[r] = fe_sub(o, sh_v[r], F);
+        sh_v[r] = o;
+      }
+      if (!skip1) acc[1] = fe_add(acc[1], shape_value<L, K>(sh_v, F, std::integral_constant<int, SHAPE>{}), F);
+#pragma unroll
+      for (int t = 2; t <= D; ++t) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) sh_v[r] = fe_add(sh_v[r], sh_d[r], F);
+        acc[t] = fe_add(acc[t], shape_value<L, K>(sh_v, F, std::integral_constant<int, SHAPE>{}), F);
+      }
+    }
   }
 }
 
@@ -437,7 +502,7 @@ __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { re
 __host__ __device__ constexpr int kernel_threads(int L) { return L >= 8 ? 128 : 256; }
 __host__ __device__ constexpr int kernel_min_blocks(int L) { return L >= 8 ? 3 : 1; }
 
-template <int L, int K, int DMAX>
+template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>
 __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
     round_kernel(const RoundArgs A, const ExprDev E, const FieldParams<L, K> F) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -457,8 +522,8 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
   Fe<L> r_prev = fe_zero<L>();
   if (A.fold) r_prev = ld_fe_cg<L>(A.st.chals + (A.round - 1) * L);
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * nthr;
-  process_pairs<L, K, DMAX>(A.src, A.dst, A.src_len, A.fold != 0, r_prev, E, sv, sd,
-                            static_cast<uint64_t>(blockIdx.x) * nthr + tid, A.pairs, stride, A.skip1 != 0, acc, F);
+  process_pairs<L, K, DMAX, SHAPE>(A.src, A.dst, A.src_len, A.fold != 0, r_prev, E, sv, sd,
+                                   static_cast<uint64_t>(blockIdx.x) * nthr + tid, A.pairs, stride, A.skip1 != 0, acc, F);
 
   // block partial -> global; the last block reduces all partials
   __syncthreads();
@@ -508,10 +573,12 @@ struct BatchItem {
 
 struct BatchTickArgs {
   const BatchRound* rounds;
-  const BatchItem* items;
+  const BatchItem* items;  // nullptr: one round, item i = pairs [i tile, (i + 1) tile)
   int32_t num_items;
   int32_t pad;
-  uint32_t* head;      // queue counter of this tick (zero before the launch)
+  uint32_t* head;          // queue counter of this tick (zero before the launch); nullptr:
+                           // block b does item b alone (grid = num_items)
+  uint64_t tile;           // pairs per item when items is nullptr
 };
 
 template <int L, int K, int DMAX>
@@ -527,15 +594,23 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
 
   const int tid = threadIdx.x, nthr = blockDim.x;
   if (tid == 0) cur_expr = nullptr;
-  for (;;) {
+  for (int pass = 0;; ++pass) {
     __syncthreads();
-    if (tid == 0) item_sm = static_cast<int>(atomicAdd(T.head, 1u));
+    if (tid == 0)
+      item_sm = T.head ? static_cast<int>(atomicAdd(T.head, 1u)) : (pass == 0 ? static_cast<int>(blockIdx.x) : T.num_items);
     __syncthreads();
     const int it = item_sm;
     if (it >= T.num_items) break;
-    const BatchItem I = T.items[it];
+    BatchItem I;
+    if (T.items) {
+      I = T.items[it];
+    } else {
+      I.round = 0;
+      I.start = static_cast<uint64_t>(it) * T.tile;
+    }
     if (tid == 0) R = T.rounds[I.round];
     __syncthreads();
+    if (!T.items) I.count = R.args.pairs - I.start < T.tile ? R.args.pairs - I.start : T.tile;
     if (R.expr != cur_expr) {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(R.expr);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&E);

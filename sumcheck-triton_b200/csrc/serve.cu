@@ -1,12 +1,18 @@
 // Served proving: a request loop with continuous batching under an HBM budget.
 //
-// One worker thread per server owns a stream, a device memory pool and the request state.
-// Each iteration of its loop
+// One worker thread per server owns two streams, a device memory pool and the request state.
+// Requests whose round 0 fills more than one wave of the GPU ("large") run whole on the
+// large-proof lane, a low-priority stream: one launch per round, one block per tile, issued
+// at admission. All others are batched continuously in ticks on high-priority streams, so
+// their blocks are dispatched ahead of the lane's as the lane's blocks retire: small proofs
+// overtake large ones on the device instead of queueing behind them, while a large proof
+// runs at the efficiency of its own full-GPU rounds. Each iteration of the worker's loop
 //   1. moves submitted requests into the arrival-order waiting queue;
 //   2. admits requests from the head of that queue while the admitted footprint stays within
 //      the budget: allocates the request's block from the pool (stream-ordered), uploads its
 //      expression, generates its tables from the seed on the device -- all queued behind the
-//      work already on the stream, so admission never waits for the GPU;
+//      work already on the stream, so admission never waits for the GPU (a large request's
+//      whole proof, result copy and free are queued on the lane right here);
 //   3. issues one tick: (request round, tile) items of one batched-round-kernel launch per
 //      degree class (classes on their own streams, forked from and joined back to the
 //      server stream). Every request whose current round has at most one wave of tiles
@@ -16,7 +22,7 @@
 //      holding its last tile finalises it (SHA3 challenge included) wherever that falls. A
 //      request whose last round was issued gets its state copied to pinned memory and its
 //      block freed (both stream-ordered) in the same tick;
-//   4. retires finished ticks (event queries) and publishes their requests' results.
+//   4. retires finished ticks and large requests (event queries) and publishes results.
 // The host runs at most kSlots ticks ahead of the GPU; tick t+1 is built while tick t runs.
 //
 // The FIFO-plain policy is the baseline: one request at a time, tables generated, then the
@@ -65,6 +71,8 @@ struct ServeRequest {
   uint32_t* tables = nullptr;
   uint32_t* fold_a = nullptr;
   uint32_t* fold_b = nullptr;
+  BatchRound* rounds_dev = nullptr;  // large requests: every round's descriptor
+  bool large = false;    // runs whole on the large-proof lane
   int slot = -1;         // pinned staging slot
   int round = 0;         // current round
   uint64_t issued = 0;   // items of the current round issued so far
@@ -90,7 +98,7 @@ struct TickSlot {
 
 // Layout of one request's device block. Offsets in bytes, every part kAlign-aligned.
 struct BlockLayout {
-  size_t state, partials, expr, tables, fold_a, fold_b, total;
+  size_t state, partials, expr, rounds, tables, fold_a, fold_b, total;
 };
 
 inline BlockLayout block_layout(int n, int K, int L, int tile_pairs) {
@@ -104,6 +112,8 @@ inline BlockLayout block_layout(int n, int K, int L, int tile_pairs) {
   off = align_up(off + std::max<uint64_t>(items0, 1) * kMaxPoints * L * 4, kAlign);
   b.expr = off;
   off = align_up(off + sizeof(ExprDev), kAlign);
+  b.rounds = off;
+  off = align_up(off + static_cast<size_t>(n) * sizeof(BatchRound), kAlign);
   b.tables = off;
   off = align_up(off + static_cast<size_t>(K) * L * N * 4, kAlign);
   b.fold_a = off;
@@ -132,6 +142,13 @@ struct sc_server {
   std::deque<int> slots_in_flight;
   uint32_t* stage_host = nullptr;  // pinned [max_inflight][stage_words] result staging
   ExprDev* expr_host = nullptr;    // pinned [max_inflight] expression staging
+  BatchRound* rounds_host = nullptr;  // pinned [max_inflight][kMaxRounds] (large requests)
+  std::vector<cudaEvent_t> stage_events;  // per staging slot: a large request's completion
+  // large-proof lane: a low-priority stream of its own, with a context for table generation
+  cudaStream_t lane = nullptr;
+  sc_ctx* lane_ctx = nullptr;
+  std::deque<ServeRequest*> lane_inflight;
+  int64_t large_items = 1;         // round-0 tiles above which a request takes the lane
   size_t stage_words = 0;
   std::vector<int> free_stage;
   int64_t wave_items = 1;          // resident blocks of the largest class grid: one wave
@@ -238,7 +255,7 @@ void mark_busy(sc_server* S) {
 }
 
 void mark_idle_if_done(sc_server* S) {
-  if (S->busy_since >= 0 && S->active.empty() && S->slots_in_flight.empty()) {
+  if (S->busy_since >= 0 && S->active.empty() && S->slots_in_flight.empty() && S->lane_inflight.empty()) {
     const double t = S->now();
     std::lock_guard<std::mutex> lk(S->mu);
     S->stats.busy_s += t - S->busy_since;
@@ -273,19 +290,89 @@ int retire_ticks(sc_server* S, bool block) {
     T.busy = false;
     S->slots_in_flight.pop_front();
   }
+  // the large-proof lane completes in admission order
+  while (!S->lane_inflight.empty()) {
+    ServeRequest* R = S->lane_inflight.front();
+    const cudaError_t q = cudaEventQuery(S->stage_events[R->slot]);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return fail(SC_ERR_CUDA, "large request: %s", cudaGetErrorString(q));
+    const double t = S->now();
+    const uint32_t* hs = S->stage_host + static_cast<size_t>(R->slot) * S->stage_words;
+    const uint32_t dev_status = hs[R->so.status];
+    extract_results(S, R, hs);
+    S->free_stage.push_back(R->slot);
+    R->slot = -1;
+    S->admitted_bytes -= R->footprint;  // its block went back to the pool before the event
+    S->lane_inflight.pop_front();
+    publish(S, R, dev_status ? SC_ERR_DEVICE : SC_OK, t);
+  }
   mark_idle_if_done(S);
   return SC_OK;
 }
 
+// A large request, whole, on the lane: state, descriptors, tables, one launch per round (one
+// block per tile, so the small requests' higher-priority launches take SMs as these blocks
+// retire), result copy, free, completion event -- all ordered on the lane.
+int issue_large(sc_server* S, ServeRequest* R) {
+  SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->lane));
+  ExprDev& E = S->expr_host[R->slot];
+  build_expr(S, R->expr, E);
+  SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->lane));
+  BatchRound* rh = S->rounds_host + static_cast<size_t>(R->slot) * kMaxRounds;
+  const uint64_t tile = static_cast<uint64_t>(S->tile_pairs);
+  for (int t = 0; t < R->n; ++t) {
+    BatchRound& B = rh[t];
+    std::memset(&B, 0, sizeof(B));
+    round_args(S, *R, t, B.args);
+    const uint64_t items = (B.args.pairs + tile - 1) / tile;
+    B.expr = R->expr_dev;
+    B.partials = R->partials;
+    B.first_item = 0;
+    B.num_items = static_cast<int32_t>(items);
+    B.item_base = 0;
+    B.round_items = static_cast<int32_t>(items);
+  }
+  SC_CUDA(cudaMemcpyAsync(R->rounds_dev, rh, static_cast<size_t>(R->n) * sizeof(BatchRound), cudaMemcpyHostToDevice,
+                          S->lane));
+  int rc = sc_tables_generate(S->lane_ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
+  if (rc) return rc;
+  int c = 0;
+  while (S->classes[c].dclass != R->dclass) ++c;
+  const ServeClass& C = S->classes[c];
+  for (int t = 0; t < R->n; ++t) {
+    BatchTickArgs A;
+    A.rounds = R->rounds_dev + t;
+    A.items = nullptr;
+    A.num_items = rh[t].num_items;
+    A.pad = 0;
+    A.head = nullptr;
+    A.tile = tile;
+    rc = batch_kernel_launch(S->L, S->kind, C.dclass, S->field, static_cast<unsigned>(A.num_items), C.threads, C.smem,
+                             S->lane, A);
+    if (rc) return rc;
+  }
+  SC_CUDA(cudaMemcpyAsync(S->stage_host + static_cast<size_t>(R->slot) * S->stage_words, R->state,
+                          R->so.total_words * 4, cudaMemcpyDeviceToHost, S->lane));
+  SC_CUDA(cudaFreeAsync(R->block, S->lane));
+  R->block = nullptr;
+  SC_CUDA(cudaEventRecord(S->stage_events[R->slot], S->lane));
+  S->lane_inflight.push_back(R);
+  return SC_OK;
+}
+
 int admit(sc_server* S) {
-  while (!S->waiting.empty() && static_cast<int>(S->active.size()) < S->max_inflight && !S->free_stage.empty()) {
+  while (!S->waiting.empty() && static_cast<int>(S->active.size() + S->lane_inflight.size()) < S->max_inflight &&
+         !S->free_stage.empty()) {
     ServeRequest* R = S->waiting.front();
     if (S->admitted_bytes + R->footprint > S->budget) break;  // arrival order: no overtaking
     S->waiting.pop_front();
     const BlockLayout b = block_layout(R->n, R->K, S->L, S->tile_pairs);
+    const uint64_t items0 = ((uint64_t{1} << R->n) / 2 + S->tile_pairs - 1) / S->tile_pairs;
+    R->large = static_cast<int64_t>(items0) > S->large_items;
+    cudaStream_t st = R->large ? S->lane : S->stream;
     void* p = nullptr;
     const double a0 = S->now();
-    const cudaError_t e = cudaMallocFromPoolAsync(&p, b.total, S->pool, S->stream);
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, b.total, S->pool, st);
     S->add_time(&sc_server_stats::alloc_s, S->now() - a0);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -296,6 +383,7 @@ int admit(sc_server* S) {
     R->state = reinterpret_cast<uint32_t*>(R->block + b.state);
     R->partials = reinterpret_cast<uint32_t*>(R->block + b.partials);
     R->expr_dev = reinterpret_cast<ExprDev*>(R->block + b.expr);
+    R->rounds_dev = reinterpret_cast<BatchRound*>(R->block + b.rounds);
     R->tables = reinterpret_cast<uint32_t*>(R->block + b.tables);
     R->fold_a = reinterpret_cast<uint32_t*>(R->block + b.fold_a);
     R->fold_b = reinterpret_cast<uint32_t*>(R->block + b.fold_b);
@@ -303,18 +391,23 @@ int admit(sc_server* S) {
     S->free_stage.pop_back();
     R->round = 0;
     R->issued = 0;
-    SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->stream));
-    ExprDev& E = S->expr_host[R->slot];
-    build_expr(S, R->expr, E);
-    SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->stream));
-    int rc = sc_tables_generate(S->ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
-    if (rc) return rc;
     R->t_admit = S->now();
     S->admitted_bytes += R->footprint;
-    S->active.push_back(R);
     mark_busy(S);
+    if (R->large) {
+      int rc = issue_large(S, R);
+      if (rc) return rc;
+    } else {
+      SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->stream));
+      ExprDev& E = S->expr_host[R->slot];
+      build_expr(S, R->expr, E);
+      SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->stream));
+      int rc = sc_tables_generate(S->ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
+      if (rc) return rc;
+      S->active.push_back(R);
+    }
     std::lock_guard<std::mutex> lk(S->mu);
-    S->stats.peak_inflight = std::max<uint64_t>(S->stats.peak_inflight, S->active.size());
+    S->stats.peak_inflight = std::max<uint64_t>(S->stats.peak_inflight, S->active.size() + S->lane_inflight.size());
     S->stats.peak_footprint = std::max<uint64_t>(S->stats.peak_footprint, S->admitted_bytes);
   }
   return SC_OK;
@@ -423,6 +516,7 @@ int issue_tick(sc_server* S, bool* issued) {
     A.num_items = static_cast<int32_t>(items[c].size());
     A.pad = 0;
     A.head = reinterpret_cast<uint32_t*>(T.dev) + c;
+    A.tile = 0;
     SC_CUDA(cudaStreamWaitEvent(C.stream, S->fork, 0));
     const unsigned grid = static_cast<unsigned>(std::min(C.grid, std::max(1, A.num_items)));
     int rc = batch_kernel_launch(S->L, S->kind, C.dclass, S->field, grid, C.threads, C.smem, C.stream, A);
@@ -459,35 +553,53 @@ void fail_all(sc_server* S, int rc) {
   const double t = S->now();
   std::vector<ServeRequest*> all(S->waiting.begin(), S->waiting.end());
   all.insert(all.end(), S->active.begin(), S->active.end());
+  all.insert(all.end(), S->lane_inflight.begin(), S->lane_inflight.end());
   for (int s = 0; s < kSlots; ++s)
     for (ServeRequest* R : S->slots[s].completing) all.push_back(R);
   S->waiting.clear();
   S->active.clear();
+  S->lane_inflight.clear();
   for (int s = 0; s < kSlots; ++s) S->slots[s].completing.clear();
   S->slots_in_flight.clear();
   for (ServeRequest* R : all) publish(S, R, rc, t);
 }
 
 void loop_continuous(sc_server* S) {
+  bool lane_only = false;  // last pass: nothing to issue, only the lane in flight
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      const bool idle = S->waiting.empty() && S->active.empty() && S->slots_in_flight.empty();
-      if (idle) S->cv_work.wait(lk, [S] { return S->stop || !S->incoming.empty(); });
+      const bool idle = S->waiting.empty() && S->active.empty() && S->slots_in_flight.empty() && S->lane_inflight.empty();
+      if (idle) {
+        S->cv_work.wait(lk, [S] { return S->stop || !S->incoming.empty(); });
+      } else if (lane_only) {
+        // poll the lane's completions, waking early for a new request
+        const double w0 = S->now();
+        S->cv_work.wait_for(lk, std::chrono::microseconds(100), [S] { return S->stop || !S->incoming.empty(); });
+        S->stats.wait_s += S->now() - w0;
+      }
       while (!S->incoming.empty()) {
         S->waiting.push_back(S->incoming.front());
         S->incoming.pop_front();
       }
-      if (S->stop && S->waiting.empty() && S->active.empty() && S->slots_in_flight.empty()) return;
+      if (S->stop && S->waiting.empty() && S->active.empty() && S->slots_in_flight.empty() && S->lane_inflight.empty())
+        return;
     }
     int rc = retire_ticks(S, false);
     if (!rc) rc = admit(S);
     bool issued = false;
     if (!rc) rc = issue_tick(S, &issued);
-    if (!rc && !issued && !S->slots_in_flight.empty()) rc = retire_ticks(S, true);
+    lane_only = false;
+    if (!rc && !issued) {
+      if (!S->slots_in_flight.empty())
+        rc = retire_ticks(S, true);
+      else
+        lane_only = !S->lane_inflight.empty();
+    }
     if (rc) {
       fail_all(S, rc);
       cudaStreamSynchronize(S->stream);
+      cudaStreamSynchronize(S->lane);
       cudaGetLastError();
     }
   }
@@ -573,12 +685,17 @@ void destroy_resources(sc_server* S) {
     if (T.dev) cudaFree(T.dev);
     if (T.done) cudaEventDestroy(T.done);
   }
+  if (S->lane) cudaStreamSynchronize(S->lane);
   if (S->fork) cudaEventDestroy(S->fork);
+  for (cudaEvent_t e : S->stage_events) cudaEventDestroy(e);
   if (S->stage_host) cudaFreeHost(S->stage_host);
   if (S->expr_host) cudaFreeHost(S->expr_host);
+  if (S->rounds_host) cudaFreeHost(S->rounds_host);
   if (S->ctx) sc_ctx_destroy(S->ctx);
+  if (S->lane_ctx) sc_ctx_destroy(S->lane_ctx);
   if (S->pool) cudaMemPoolDestroy(S->pool);
   if (S->stream) cudaStreamDestroy(S->stream);
+  if (S->lane) cudaStreamDestroy(S->lane);
 }
 
 }  // namespace
@@ -616,9 +733,14 @@ int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm
     destroy_resources(S.get());
     return rc;
   };
-  cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+  // priorities: the small requests' ticks above the large-proof lane
+  int prio_low = 0, prio_high = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&S->stream, cudaStreamNonBlocking, prio_high);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&S->lane, cudaStreamNonBlocking, prio_low);
   if (e != cudaSuccess) return bail(fail(SC_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
   int rc = sc_ctx_create(device, S->stream, &S->ctx);
+  if (!rc) rc = sc_ctx_create(device, S->lane, &S->lane_ctx);
   if (rc) return bail(rc);
   cudaMemPoolProps props;
   std::memset(&props, 0, sizeof(props));
@@ -629,6 +751,10 @@ int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm
   if (e != cudaSuccess) return bail(fail(SC_ERR_CUDA, "memory pool: %s", cudaGetErrorString(e)));
   uint64_t keep = ~uint64_t{0};  // freed blocks stay mapped in the pool for the next request
   e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  // a block freed on the lane is reused by the other stream only once its free completed:
+  // no dependency that would hold small requests behind the lane
+  int no = 0;
+  if (e == cudaSuccess) e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
   if (e != cudaSuccess) return bail(fail(SC_ERR_CUDA, "memory pool attribute: %s", cudaGetErrorString(e)));
   // one tile size for every class (a request's partial slots are sized by it)
   int cls_threads = kernel_threads(S->L);
@@ -644,12 +770,13 @@ int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm
                                  &C.smem)))
       return bail(rc);
     max_grid = std::max(max_grid, C.grid);
-    e = cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithPriority(&C.stream, cudaStreamNonBlocking, prio_high);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&C.done, cudaEventDisableTiming);
     S->classes.push_back(C);
     if (e != cudaSuccess) return bail(fail(SC_ERR_CUDA, "class stream: %s", cudaGetErrorString(e)));
   }
   S->wave_items = max_grid;
+  S->large_items = max_grid;
   S->tick_budget = chunk_items ? chunk_items : 2 * max_grid;
   S->tick_item_cap = static_cast<int>(std::max<int64_t>(8 * max_grid, 2 * S->tick_budget));
   e = cudaEventCreateWithFlags(&S->fork, cudaEventDisableTiming);
@@ -666,6 +793,13 @@ int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm
   S->stage_words = align_up(state_offsets(kMaxRounds, max_tables, S->L).total_words, 64);
   e = cudaMallocHost(&S->stage_host, static_cast<size_t>(max_inflight) * S->stage_words * 4);
   if (e == cudaSuccess) e = cudaMallocHost(&S->expr_host, static_cast<size_t>(max_inflight) * sizeof(ExprDev));
+  if (e == cudaSuccess)
+    e = cudaMallocHost(&S->rounds_host, static_cast<size_t>(max_inflight) * kMaxRounds * sizeof(BatchRound));
+  for (int i = 0; e == cudaSuccess && i < max_inflight; ++i) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) S->stage_events.push_back(ev);
+  }
   if (e != cudaSuccess) return bail(fail(SC_ERR_NOMEM, "pinned staging: %s", cudaGetErrorString(e)));
   for (int i = max_inflight - 1; i >= 0; --i) S->free_stage.push_back(i);
   sc_server* raw = S.release();

@@ -3,9 +3,11 @@
 ``ProofServer`` wraps ``sc_server_*``: a native worker thread that admits requests in
 arrival order by their HBM footprint, keeps each admitted request's tables (generated on
 the device from its seed), fold buffers and transcript state resident, and merges the
-rounds of all in-flight requests into shared launches of the batched round kernel. Large
-rounds advance a chunk of tiles per launch, so requests that arrive while a large proof
-runs overlap with it instead of queueing behind it. Policy ``"fifo_plain"`` is the
+rounds of the in-flight requests into shared launches of the batched round kernel on
+high-priority streams. A request whose first round is larger than one wave of the GPU runs
+whole on a low-priority stream instead (one launch per round, one block per tile), so the
+small requests' blocks take SMs as its blocks retire: requests that arrive while a large
+proof runs overtake it instead of queueing behind it. Policy ``"fifo_plain"`` is the
 baseline: one request at a time, in arrival order, through the plain per-round path.
 
 A request's result is bit-identical to ``prove_device`` on ``generate_tables`` with the

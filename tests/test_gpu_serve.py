@@ -84,6 +84,21 @@ def test_requests_joining_while_others_run():
         assert any(srv.times(r).done_s < tb.done_s for r in ids)
 
 
+def test_large_requests_on_their_lane_with_small_ones():
+    large = _stream(3, 20, 21, 71)
+    small = _stream(16, 3, 12, 72)
+    with ProofServer(SPEC) as srv:
+        ids_l = [srv.submit(s.expression, s.num_vars, s.seed) for s in large]
+        ids_s = [srv.submit(s.expression, s.num_vars, s.seed) for s in small]
+        srv.drain(timeout_ms=120_000)
+        for rid, s in zip(ids_l + ids_s, large + small):
+            _same(srv.result(rid), _alone(SPEC, s))
+        # the small requests overtook the large ones submitted before them
+        last_large = max(srv.times(r).done_s for r in ids_l)
+        assert max(srv.times(r).done_s for r in ids_s) < last_large
+        assert srv.stats()["peak_inflight"] >= 4
+
+
 def test_served_results_match_oracle():
     specs = _stream(5, 2, 6, 31)
     with ProofServer(SPEC) as srv:
