@@ -16,8 +16,8 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
-LIB = PKG / "zkduel_b200" / "libsumcheck_b200.so"
-OBJ = PKG / "_build"
+LIB = Path(os.environ.get("SC_LIB_OUT", PKG / "zkduel_b200" / "libsumcheck_b200.so"))
+OBJ = Path(os.environ.get("SC_BUILD_DIR", PKG / "_build"))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "serve.cu"]
@@ -47,7 +47,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         obj = OBJ / (src.stem + ".o")
         if not force and not _stale(obj, [src] + headers):
             continue
-        cmd = [nvcc, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-c", str(src), "-o", str(obj)]
+        extra = os.environ.get("SC_NVCC_FLAGS", "").split()
+        cmd = [nvcc, *ARCH, *FLAGS, *extra, *(["-Xptxas", "-v"] if verbose else []), "-c", str(src), "-o", str(obj)]
         procs.append((src, subprocess.Popen(cmd)))
     failed = [str(src) for src, p in procs if p.wait() != 0]
     if failed:

@@ -498,12 +498,23 @@ __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { re
 
 // Launch shape per limb count: 8-limb kernels hold (DMAX + 1) x 8-word point arrays per
 // thread, so they run 128-thread blocks and ask the compiler for at least 3 blocks per SM
-// (<= 170 registers); smaller fields run 256-thread blocks.
+// (<= 168 registers; on B200 the mixed 512-proof stream ran 10% slower with 2 or 4);
+// smaller fields run 256-thread blocks.
 __host__ __device__ constexpr int kernel_threads(int L) { return L >= 8 ? 128 : 256; }
-__host__ __device__ constexpr int kernel_min_blocks(int L) { return L >= 8 ? 3 : 1; }
+#ifndef SC_L8_MIN_BLOCKS
+#define SC_L8_MIN_BLOCKS 3
+#endif
+__host__ __device__ constexpr int kernel_min_blocks(int L) { return L >= 8 ? SC_L8_MIN_BLOCKS : 1; }
+#ifndef SC_SHAPE_MIN_BLOCKS
+#define SC_SHAPE_MIN_BLOCKS 3
+#endif
+// Shape kernels of the 1- and 2-limb fields are memory-bound: ask for more resident blocks.
+__host__ __device__ constexpr int round_min_blocks(int L, int shape) {
+  return (shape != 0 && L <= 2) ? SC_SHAPE_MIN_BLOCKS : kernel_min_blocks(L);
+}
 
 template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>
-__global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
+__global__ void __launch_bounds__(kernel_threads(L), round_min_blocks(L, SHAPE))
     round_kernel(const RoundArgs A, const ExprDev E, const FieldParams<L, K> F) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];

@@ -319,11 +319,22 @@ int issue_large(sc_server* S, ServeRequest* R) {
   build_expr(S, R->expr, E);
   SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->lane));
   BatchRound* rh = S->rounds_host + static_cast<size_t>(R->slot) * kMaxRounds;
-  const uint64_t tile = static_cast<uint64_t>(S->tile_pairs);
+  int c = 0;
+  while (S->classes[c].dclass != R->dclass) ++c;
+  const ServeClass& C = S->classes[c];
+  // A round's tile: the base tile, or larger so that the round is about kLaneWaves waves of
+  // blocks (fewer blocks, less per-block reduction and launch work; the small requests'
+  // blocks still find SMs within microseconds, as hundreds of lane blocks retire in turn).
+  constexpr uint64_t kLaneWaves = 4;
+  std::vector<uint64_t> tiles(R->n);
   for (int t = 0; t < R->n; ++t) {
     BatchRound& B = rh[t];
     std::memset(&B, 0, sizeof(B));
     round_args(S, *R, t, B.args);
+    const uint64_t want = B.args.pairs / (kLaneWaves * static_cast<uint64_t>(S->wave_items));
+    const uint64_t thr = static_cast<uint64_t>(C.threads);
+    const uint64_t tile = std::max<uint64_t>(S->tile_pairs, (want + thr - 1) / thr * thr);
+    tiles[t] = tile;
     const uint64_t items = (B.args.pairs + tile - 1) / tile;
     B.expr = R->expr_dev;
     B.partials = R->partials;
@@ -336,9 +347,6 @@ int issue_large(sc_server* S, ServeRequest* R) {
                           S->lane));
   int rc = sc_tables_generate(S->lane_ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
   if (rc) return rc;
-  int c = 0;
-  while (S->classes[c].dclass != R->dclass) ++c;
-  const ServeClass& C = S->classes[c];
   for (int t = 0; t < R->n; ++t) {
     BatchTickArgs A;
     A.rounds = R->rounds_dev + t;
@@ -346,7 +354,7 @@ int issue_large(sc_server* S, ServeRequest* R) {
     A.num_items = rh[t].num_items;
     A.pad = 0;
     A.head = nullptr;
-    A.tile = tile;
+    A.tile = tiles[t];
     rc = batch_kernel_launch(S->L, S->kind, C.dclass, S->field, static_cast<unsigned>(A.num_items), C.threads, C.smem,
                              S->lane, A);
     if (rc) return rc;
