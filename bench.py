@@ -216,6 +216,17 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def profiled_traffic_ratio(L: int):
+    """DRAM bytes / algorithmic bytes of the L-limb ticks, from the committed ncu summary."""
+    import re
+
+    f = ROOT / "profiles" / "batch_round_kernel_mixed_stream_64.md"
+    if L != 8 or not f.exists():
+        return None
+    m = re.search(r"traffic_ratio_L8:\s*([0-9.]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
 def sum_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
@@ -452,6 +463,13 @@ def main() -> int:
             roof = {"bound": "hbm", "kernel": kname, "achieved": ach, "peak": hbm_peak,
                     "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None,
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+        ratio = profiled_traffic_ratio(L) if path == "batched" else None
+        if ratio is not None:
+            roof["traffic"] = ratio * c["bytes"] / max(1, c["launches"])
+            roof["traffic_unit"] = "bytes per launch"
+            roof["traffic_source"] = (f"dram__bytes_read.sum + dram__bytes_write.sum of every {L}-limb tick of the "
+                                      f"64-proof cut (profiles/), {ratio:.3f} x the algorithmic bytes, applied to "
+                                      f"this run's algorithmic bytes per launch")
         roof["by_class"] = {f"L{k}": {"busy_ms": v["ms"], "launches": v["launches"],
                                       "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                       "TIMAD/s": v["imad"] / (v["ms"] / 1e3) / 1e12} for k, v in per_class.items()}
