@@ -526,7 +526,7 @@ def served_measure(args, device, rank: int, world: int) -> dict:
     cal = served_stream(1000, rate_per_s=1e9, seed=1000 + rank)
     with ProofServer(spec, policy="fifo_plain", budget_bytes=SERVED_BUDGET, device=dev) as srv:
         srv.reserve(reserve)
-        replay(srv, cal[:30])
+        replay(srv, sorted(cal[:100], key=lambda r: r.spec.num_vars))
         b0 = srv.stats()["busy_s"]
         replay(srv, cal)
         service_s = (srv.stats()["busy_s"] - b0) / len(cal)
@@ -540,6 +540,13 @@ def served_measure(args, device, rank: int, world: int) -> dict:
         with ProofServer(spec, policy=pol, budget_bytes=SERVED_BUDGET, device=dev) as srv:
             srv.reserve(reserve)
             replay(srv, served_stream(50, rate_per_s=rate, seed=99))
+            srv.reserve(reserve)
+            # every size once, largest last, so no scratch grows inside the timed replay
+            warm = sorted(served_stream(400, rate_per_s=1e9, seed=98), key=lambda r: r.spec.num_vars)
+            seen = {}
+            for r in warm:
+                seen[(r.spec.num_vars, r.spec.degree > 4)] = r
+            replay(srv, list(seen.values()))
             rep, kept = replay(srv, reqs, keep_results=check)
         summ = rep.summary()
         # bit-exactness on a sample: the served result equals the proof alone
