@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--path", choices=["batched", "plain"], default="batched")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuned ones")
     ap.add_argument("--served", type=int, default=SERVED_COUNT,
                     help="requests in the served stream (0: skip the served measurement)")
     ap.add_argument("--case", default=None,
@@ -371,7 +372,13 @@ def main() -> int:
 
     from zkduel_b200.batch import BatchProver
 
-    batcher = BatchProver([(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items], device=device)
+    tuning = None
+    batch_items = [(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items]
+    if not args.no_tune:
+        from zkduel_b200.autotune import tune_for
+
+        tuning = tune_for(batch_items, device=device)  # on this stream, before the timed region
+    batcher = BatchProver(batch_items, device=device, tuning=tuning)
     steps_fn = {"batched": batcher.run, "plain": lambda: run_plain(work)}
 
     def measure(path, steps):
@@ -485,6 +492,10 @@ def main() -> int:
                   "path": "one proof at a time (sc_prove per proof)"},
         "speedup_vs_plain": ms_plain / ms_step if path == "batched" else 1.0,
         "gpu_launches": gpu_launches,
+        "tuning": None if tuning is None else {"threads": tuning.to_json()["threads"],
+                                               "pairs_per_thread": tuning.to_json()["pairs_per_thread"],
+                                               "untuned_ms": tuning.timings.get("start"),
+                                               "tuned_ms": tuning.timings.get("best")},
         "clocks": clocks.summary(),
         "imad_peak_tera_per_s": imad_rate / 1e12,
     }

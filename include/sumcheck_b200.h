@@ -182,6 +182,15 @@ typedef struct sc_batch sc_batch;
 int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
                     const int32_t* num_rounds, const uint32_t* const* tables_dev,
                     int challenge_mode, int threads, int pairs_per_thread, sc_batch** out);
+/* The same with tiles chosen per degree class and per proof (what the autotuner drives):
+ * class_threads[3] = threads per block of the degree classes <= 2, <= 4, <= 7 (0: default);
+ * proof_pairs_per_thread[count] = each proof's tile, threads x pairs_per_thread pairs per
+ * work item (0: 2). Either array may be NULL (all defaults). No counterpart in the reference,
+ * as sc_batch_create. */
+int sc_batch_create_tiled(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
+                          const int32_t* num_rounds, const uint32_t* const* tables_dev,
+                          int challenge_mode, const int32_t* class_threads,
+                          const int32_t* proof_pairs_per_thread, sc_batch** out);
 /* Enqueues one run after the work queued on the context's stream (the context's stream
  * then waits for it). Asynchronous. */
 int sc_batch_run(sc_batch* batch);

@@ -18,6 +18,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = Path(os.environ.get("SC_LIB_OUT", PKG / "zkduel_b200" / "libsumcheck_b200.so"))
 OBJ = Path(os.environ.get("SC_BUILD_DIR", PKG / "_build"))
+CLI = PKG / "bin" / "field_sumcheck_b200"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "serve.cu"]
@@ -35,9 +36,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     hdr = CSRC / "field_ptx.cuh"
     if _stale(hdr, [gen]):
         subprocess.check_call([sys.executable, str(gen)])
+    gen_w = CSRC / "gen_workload_table.py"
+    hdr_w = CSRC / "workload_table.h"
+    if _stale(hdr_w, [gen_w, PKG / "zkduel_b200" / "workloads.py", PKG / "zkduel_b200" / "fields.py"]):
+        subprocess.check_call([sys.executable, str(gen_w)])
     sources = [CSRC / s for s in SOURCES]
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "sumcheck_b200.h"]
     if not force and not _stale(LIB, sources + headers):
+        build_cli(os.environ.get("NVCC", "nvcc"))
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     OBJ.mkdir(exist_ok=True)
@@ -55,7 +61,20 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         raise subprocess.CalledProcessError(1, f"nvcc {' '.join(failed)}")
     objs = [str(OBJ / (src.stem + ".o")) for src in sources]
     subprocess.check_call([nvcc, *ARCH, "-shared", *objs, "-o", str(LIB)])
+    build_cli(nvcc)
     return LIB
+
+
+def build_cli(nvcc: str = "nvcc") -> Path:
+    """The reference executable's command line over this library (cli/field_sumcheck_b200.cpp)."""
+    src = PKG / "cli" / "field_sumcheck_b200.cpp"
+    if not CLI.parent.exists():
+        CLI.parent.mkdir(parents=True)
+    if _stale(CLI, [src, LIB, CSRC / "workload_table.h", PKG.parent / "include" / "sumcheck_b200.h"]):
+        rpath = "$ORIGIN/" + os.path.relpath(LIB.parent, CLI.parent)
+        subprocess.check_call([nvcc, *ARCH, "-O2", "-std=c++17", str(src), "-o", str(CLI), "-L", str(LIB.parent),
+                               "-l" + LIB.stem[3:], "-Xlinker", "-rpath", "-Xlinker", rpath])
+    return CLI
 
 
 if __name__ == "__main__":

@@ -42,7 +42,8 @@ struct sc_batch {
   int L = 0, kind = 0;
   int count = 0;
   int mode = 0;
-  int threads_req = 0, ppt = 2;
+  int class_threads[3] = {0, 0, 0};  // requested threads per block, degree classes 2, 4, 7 (0: default)
+  std::vector<int> ppt;               // pairs per thread of each proof's tiles
   std::vector<int> n, K, d;
   std::vector<StateOffsets> so;
   std::vector<size_t> state_base;  // word offset of each proof's state
@@ -140,7 +141,9 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
         C.max_rounds = std::max(C.max_rounds, B->n[p]);
       }
     if (C.proofs.empty()) continue;
-    if ((rc = batch_kernel_setup(L, B->kind, dc, kmax, B->threads_req, ctx->sm_count, &C.threads, &C.grid, &C.smem)))
+    const int ci = dc == 2 ? 0 : (dc == 4 ? 1 : 2);
+    if ((rc = batch_kernel_setup(L, B->kind, dc, kmax, B->class_threads[ci], ctx->sm_count, &C.threads, &C.grid,
+                                 &C.smem)))
       return rc;
     B->classes.push_back(std::move(C));
   }
@@ -211,7 +214,7 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
         A.st.claim0 = s + o.claim0;
         A.st.claim = s + o.claim;
         R.expr = exprs_dev + p;
-        const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt;
+        const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt[p];
         const uint64_t nitems = (A.pairs + tile - 1) / tile;
         R.first_item = static_cast<int>(items.size()) - C.tick_item0[t];  // tick-relative
         R.num_items = static_cast<int>(nitems);
@@ -275,17 +278,20 @@ int batch_issue(sc_batch* B) {
 
 extern "C" {
 
-int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
-                    const int32_t* num_rounds, const uint32_t* const* tables_dev, int challenge_mode,
-                    int threads, int pairs_per_thread, sc_batch** out) {
+int sc_batch_create_tiled(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
+                          const int32_t* num_rounds, const uint32_t* const* tables_dev, int challenge_mode,
+                          const int32_t* class_threads, const int32_t* proof_pairs_per_thread, sc_batch** out) {
   if (!ctx || !field || !exprs || !num_rounds || !tables_dev || !out) return fail(SC_ERR_INVALID, "NULL argument");
   *out = nullptr;
   if (count < 1) return fail(SC_ERR_INVALID, "empty batch");
   if (challenge_mode != SC_CHALLENGE_SHA3 && challenge_mode != SC_CHALLENGE_FIXED)
     return fail(SC_ERR_INVALID, "batches derive their challenges: SHA3 or fixed mode");
-  if (threads != 0 && (threads < 32 || threads > 256 || threads % 32))
-    return fail(SC_ERR_INVALID, "threads must be 0 (auto) or a multiple of 32 in 32..256");
-  if (pairs_per_thread < 0 || pairs_per_thread > 64) return fail(SC_ERR_INVALID, "pairs_per_thread outside 0..64");
+  for (int c = 0; class_threads && c < 3; ++c)
+    if (class_threads[c] != 0 && (class_threads[c] < 32 || class_threads[c] > 256 || class_threads[c] % 32))
+      return fail(SC_ERR_INVALID, "class_threads[%d] must be 0 (auto) or a multiple of 32 in 32..256", c);
+  for (int p = 0; proof_pairs_per_thread && p < count; ++p)
+    if (proof_pairs_per_thread[p] < 0 || proof_pairs_per_thread[p] > 64)
+      return fail(SC_ERR_INVALID, "proof %d: pairs_per_thread outside 0..64", p);
   for (int p = 0; p < count; ++p) {
     if (!exprs[p] || !tables_dev[p]) return fail(SC_ERR_INVALID, "proof %d: NULL expression or tables", p);
     if (num_rounds[p] < 1 || num_rounds[p] > kMaxRounds) return fail(SC_ERR_INVALID, "proof %d: num_rounds %d", p, num_rounds[p]);
@@ -300,8 +306,11 @@ int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr
   B->kind = field_kind(field->hf.p, B->L);
   B->count = count;
   B->mode = challenge_mode;
-  B->threads_req = threads;
-  B->ppt = pairs_per_thread ? pairs_per_thread : 2;
+  for (int c = 0; c < 3; ++c) B->class_threads[c] = class_threads ? class_threads[c] : 0;
+  for (int p = 0; p < count; ++p) {
+    const int v = proof_pairs_per_thread ? proof_pairs_per_thread[p] : 0;
+    B->ppt.push_back(v ? v : 2);
+  }
   for (int p = 0; p < count; ++p) B->n.push_back(num_rounds[p]);
   int rc;
   switch (B->L) {
@@ -333,6 +342,18 @@ int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr
   }
   *out = B;
   return SC_OK;
+}
+
+int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr* const* exprs,
+                    const int32_t* num_rounds, const uint32_t* const* tables_dev, int challenge_mode,
+                    int threads, int pairs_per_thread, sc_batch** out) {
+  if (threads != 0 && (threads < 32 || threads > 256 || threads % 32))
+    return fail(SC_ERR_INVALID, "threads must be 0 (auto) or a multiple of 32 in 32..256");
+  if (pairs_per_thread < 0 || pairs_per_thread > 64) return fail(SC_ERR_INVALID, "pairs_per_thread outside 0..64");
+  if (count < 1) return fail(SC_ERR_INVALID, "empty batch");
+  const int32_t ct[3] = {threads, threads, threads};
+  std::vector<int32_t> ppt(static_cast<size_t>(count), pairs_per_thread);
+  return sc_batch_create_tiled(ctx, field, count, exprs, num_rounds, tables_dev, challenge_mode, ct, ppt.data(), out);
 }
 
 int sc_batch_run(sc_batch* B) {

@@ -84,6 +84,11 @@ SIGNATURES = {
         [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_int32), POINTER(c_void_p), c_int, c_int, c_int,
          POINTER(c_void_p)],
     ),
+    "sc_batch_create_tiled": (
+        c_int,
+        [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_int32), POINTER(c_void_p), c_int, POINTER(c_int32),
+         POINTER(c_int32), POINTER(c_void_p)],
+    ),
     "sc_batch_run": (c_int, [c_void_p]),
     "sc_batch_wait": (c_int, [c_void_p]),
     "sc_batch_result": (c_int, [c_void_p, c_int, U32P, U32P, U32P, U32P, U64P]),

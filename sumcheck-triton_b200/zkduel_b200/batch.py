@@ -24,6 +24,11 @@ from .expression import encode_expression
 from .fields import FieldSpec, get_field
 
 
+def degree_class(d: int) -> int:
+    """The kernel class that proves degree d (its register arrays hold class + 1 points)."""
+    return 2 if d <= 2 else (4 if d <= 4 else 7)
+
+
 @dataclass
 class _Group:
     spec: FieldSpec
@@ -38,10 +43,13 @@ class BatchProver:
     ``tables`` are device tensors (K, L, 2^n) of Montgomery limbs (``generate_tables`` /
     ``upload_tables``); they must stay alive while the prover exists.
     ``tile`` maps a limb count to (threads per block, pairs per thread); None = defaults.
+    ``tuning`` (an ``autotune.TuneTable``) chooses threads per (field, degree class) and pairs
+    per thread per (field, degree class, num_vars); it overrides ``tile``.
     """
 
     def __init__(self, items: Sequence[tuple], device=None, challenge_mode: str = "sha3",
-                 tile: dict[int, tuple[int, int]] | None = None, fields: Sequence[FieldSpec] | None = None):
+                 tile: dict[int, tuple[int, int]] | None = None, fields: Sequence[FieldSpec] | None = None,
+                 tuning=None):
         lib = _lib.load()
         self.ctx = get_context(device)
         self.items = list(items)
@@ -72,10 +80,17 @@ class BatchProver:
                 if tuple(t.shape) != want or not t.is_contiguous():
                     raise ValueError(f"proof {i}: tables {tuple(t.shape)}, expected contiguous {want}")
             threads, ppt = (tile or {}).get(L, (0, 0))
+            cls_threads = [int(threads)] * 3
+            proof_ppt = [int(ppt)] * n
+            if tuning is not None:
+                cls_threads = [tuning.threads(L, dc) for dc in (2, 4, 7)]
+                proof_ppt = [tuning.pairs_per_thread(L, degree_class(e.degree), int(self.items[i][2]))
+                             for i, e in zip(idx, exprs)]
             h = ctypes.c_void_p()
-            rc = lib.sc_batch_create(self.ctx.handle, fld.handle, n, expr_arr, rounds, tabs, mode,
-                                     int(threads), int(ppt), ctypes.byref(h))
-            _lib.check(rc, "sc_batch_create")
+            rc = lib.sc_batch_create_tiled(self.ctx.handle, fld.handle, n, expr_arr, rounds, tabs, mode,
+                                           (ctypes.c_int32 * 3)(*cls_threads), (ctypes.c_int32 * n)(*proof_ppt),
+                                           ctypes.byref(h))
+            _lib.check(rc, "sc_batch_create_tiled")
             self.groups.append(_Group(spec, idx, exprs, h))
             self._keep.append((expr_arr, rounds, tabs))
 

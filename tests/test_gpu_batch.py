@@ -94,3 +94,44 @@ def test_fixed_mode_and_rejects_explicit():
         _same(bp.result(i), api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "fixed"))
     with pytest.raises(ValueError):
         BatchProver(items, challenge_mode="explicit")
+
+
+def test_tuned_tiles_are_bit_identical():
+    from zkduel_b200.autotune import TuneTable
+
+    specs = _mixed(30, 2, 12, 13)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    rng = random.Random(5)
+    tune = TuneTable()
+    for L in (2, 8):
+        for dc in (2, 4, 7):
+            tune.threads_by[(L, dc)] = rng.choice([32, 64, 128, 256])
+            for r in range(4):
+                tune.ppt_by[(L, dc, r)] = rng.choice([1, 2, 3, 8, 16])
+    bp = BatchProver(items, tuning=tune)
+    bp.run()
+    for i, s in enumerate(specs):
+        _same(bp.result(i), api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
+
+
+def test_autotune_fills_its_table(tmp_path):
+    from zkduel_b200 import autotune as A
+
+    t = A.load_or_tune((64,), cache=tmp_path / "tune.json", proofs_per_range=2, reps=1)
+    assert all(t.threads(2, dc) in A.THREADS for dc in A.CLASSES)
+    assert all(t.pairs_per_thread(2, dc, n) in A.PAIRS_PER_THREAD for dc in A.CLASSES for n in (10, 14, 17, 19))
+    again = A.load_or_tune((64,), cache=tmp_path / "tune.json")  # from the cache: no timing
+    assert again.threads_by == t.threads_by and again.ppt_by == t.ppt_by
+
+
+def test_tune_for_keeps_results_and_reports_timings():
+    from zkduel_b200.autotune import tune_for
+
+    specs = _mixed(16, 4, 12, 17)
+    items = [(s.expression, s.bit_width, s.num_vars, _tables(get_field(s.bit_width), s)) for s in specs]
+    t = tune_for(items, reps=1, ppt_candidates=(1, 4))
+    assert t.timings["best"] <= t.timings["start"]
+    bp = BatchProver(items, tuning=t)
+    bp.run()
+    for i, s in enumerate(specs):
+        _same(bp.result(i), api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
