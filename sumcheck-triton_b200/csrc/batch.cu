@@ -63,6 +63,7 @@ namespace {
 template <int L, int K, int D>
 struct KernelSetup {
   static int run(int kmax, int threads_req, int sm_count, int* threads_out, int* grid_out, size_t* smem_out) {
+
     int threads = std::min(threads_req ? threads_req : kernel_threads(L), kernel_threads(L));
     const int per_thread = round_smem_words_per_thread(kmax, L) * 4;
     while (threads > 32 && static_cast<size_t>(threads) * per_thread > static_cast<size_t>(kMaxDynSmem)) threads -= 32;

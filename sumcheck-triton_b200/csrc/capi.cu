@@ -6,6 +6,7 @@
 // (cuda/src/field_sumcheck.cu:1012-1088); here a proof is num_rounds launches of one
 // fused round kernel on the caller's stream and a single copy of the results at the end.
 #include "host_common.h"
+#include "prover_pp.cuh"
 
 using namespace sc;
 using namespace sc_host;
@@ -48,7 +49,12 @@ struct ProveRun {
     }
     int threads = kernel_threads(L);
     size_t smem;
-    if (shape == kShapeGeneric) {
+    if (use_point_parallel(L) && shape == kShapeGeneric) {
+      kern = round_kernel_pp<L, K>;
+      threads = kPointParallelThreads;
+      smem = static_cast<size_t>(pp_smem_words(threads, K_, L)) * 4;
+      SC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    } else if (shape == kShapeGeneric) {
       const int per_thread = round_smem_words_per_thread(K_, L) * 4;
       while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
       smem = static_cast<size_t>(threads) * per_thread;
@@ -103,7 +109,13 @@ struct ProveRun {
         A.dst = static_cast<uint32_t*>((j & 1) ? ctx->fold_a.p : ctx->fold_b.p);
         prev = A.dst;
       }
-      const uint64_t want = (A.pairs + threads - 1) / threads;
+      uint64_t per_block = static_cast<uint64_t>(threads);
+      if (use_point_parallel(L) && shape == kShapeGeneric) {  // pairs a block holds: one per lane group
+        const int npts = ex->degree + 1 - (A.skip1 ? 1 : 0);
+        const int G = npts <= 2 ? 2 : (npts <= 4 ? 4 : 8);
+        per_block = static_cast<uint64_t>(threads / G);
+      }
+      const uint64_t want = (A.pairs + per_block - 1) / per_block;
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, grid_max));
       cudaEvent_t ev;
       if ((rc = timing_begin(ctx, &ev))) return rc;

@@ -501,6 +501,13 @@ __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { re
 // (<= 168 registers; on B200 the mixed 512-proof stream ran 10% slower with 2 or 4);
 // smaller fields run 256-thread blocks.
 __host__ __device__ constexpr int kernel_threads(int L) { return L >= 8 ? 128 : 256; }
+#ifndef SC_PP_MIN_LIMBS
+#define SC_PP_MIN_LIMBS 8
+#endif
+// Fields of at least this many limbs evaluate generic expressions point-parallel
+// (prover_pp.cuh) in the plain round kernel.
+__host__ __device__ constexpr bool use_point_parallel(int L) { return L >= SC_PP_MIN_LIMBS; }
+constexpr int kPointParallelThreads = 128;
 #ifndef SC_L8_MIN_BLOCKS
 #define SC_L8_MIN_BLOCKS 3
 #endif
