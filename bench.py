@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuned ones")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference CUDA executable comparison")
     ap.add_argument("--served", type=int, default=SERVED_COUNT,
                     help="requests in the served stream (0: skip the served measurement)")
     ap.add_argument("--case", default=None,
@@ -508,6 +509,8 @@ def main() -> int:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0, sample_stride=4)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
                                 "sample": f"{done} proofs (every 4th of the 512-proof stream), {spent:.1f} s"}
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        line["reference_cuda"] = reference_cuda_compare()
     if args.served > 0:
         del batcher, steps_fn, work
         torch.cuda.empty_cache()
@@ -519,6 +522,39 @@ def main() -> int:
 
         dist.destroy_process_group()
     return 0
+
+
+REF_BIN = ROOT / "oracle" / "_ref" / "field_sumcheck_cuda"
+CLI_BIN = ROOT / "sumcheck-triton_b200" / "bin" / "field_sumcheck_b200"
+PLAIN_CASES = (("poly_ab", 16, 32), ("zk_vanilla_zerocheck_hp", 24, 64), ("poly_abcg_plus_deg", 22, 256))
+
+
+def reference_cuda_compare() -> dict:
+    """The three plain configs through the reference's own CUDA executable (built from its
+    source for sm_100a into oracle/_ref) and through this library's drop-in of that executable,
+    same arguments and inputs (the reference's table fill): median ms of 10 runs after 2
+    warm-ups, and whether the checksums agree."""
+    import csv as _csv
+    import tempfile
+
+    if not REF_BIN.exists() or not CLI_BIN.exists():
+        return {"unavailable": "reference CUDA executable not built (oracle/Makefile.ref)"}
+    out = {"args": "--challenge-mode sha3 --point-mode specialized --warmups 2 --repeats 10 (host timer, median)"}
+    with tempfile.TemporaryDirectory() as td:
+        for wl, n, bw in PLAIN_CASES:
+            row = {}
+            for name, binary in (("reference", REF_BIN), ("b200", CLI_BIN)):
+                csv_path = Path(td) / f"{name}_{wl}.csv"
+                subprocess.run([str(binary), "--workloads", wl, "--rounds", str(n), "--bit-widths", str(bw),
+                                "--challenge-mode", "sha3", "--point-mode", "specialized", "--warmups", "2",
+                                "--repeats", "10", "--out", str(csv_path)], check=True, stdout=subprocess.DEVNULL,
+                               timeout=600)
+                r = list(_csv.DictReader(csv_path.open()))[-1]
+                row[name] = {"median_ms": float(r["median_ms"]), "checksum": int(r["checksum"])}
+            row["speedup"] = row["reference"]["median_ms"] / row["b200"]["median_ms"]
+            row["checksums_equal"] = row["reference"]["checksum"] == row["b200"]["checksum"]
+            out[f"{wl} n={n} {bw}-bit"] = row
+    return out
 
 
 def served_measure(args, device, rank: int, world: int) -> dict:

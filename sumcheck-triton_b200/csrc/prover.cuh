@@ -268,14 +268,20 @@ __device__ __forceinline__ Fe<L> shape_value(const Fe<L> (&v)[6], const FieldPar
 // point sums into acc. Generic: every table's value and difference go to this block's
 // [K][L][nthr] shared arrays sv / sd for eval_pair. Shape kernels keep them in registers
 // (tables read in role order) and evaluate the shape's compile-time formula at each point.
+#ifndef SC_PAIR_UNROLL
+#define SC_PAIR_UNROLL 1
+#endif
+constexpr int kPairUnroll = SC_PAIR_UNROLL;
 template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>
-__device__ __forceinline__ void process_pairs(const uint32_t* src, uint32_t* dst, uint64_t src_len, bool fold,
+__device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                              uint64_t src_len, bool fold,
                                               const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
                                               uint64_t first, uint64_t last, uint64_t stride, bool skip1,
                                               Fe<L> (&acc)[DMAX + 1], const FieldParams<L, K>& F) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
   const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
+#pragma unroll(SHAPE == kShapeGeneric ? 1 : kPairUnroll)
   for (uint64_t q = first; q < last; q += stride) {
     Fe<L> sh_v[NR], sh_d[NR];
 #pragma unroll (SHAPE == kShapeGeneric ? 1 : NR)
