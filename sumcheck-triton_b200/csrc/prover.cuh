@@ -268,6 +268,12 @@ __device__ __forceinline__ Fe<L> shape_value(const Fe<L> (&v)[6], const FieldPar
 // point sums into acc. Generic: every table's value and difference go to this block's
 // [K][L][nthr] shared arrays sv / sd for eval_pair. Shape kernels keep them in registers
 // (tables read in role order) and evaluate the shape's compile-time formula at each point.
+// 2-limb shape kernels issue every load of a pair before its folds and run 2 blocks/SM
+// (<= 128 registers for the loaded words): measured on B200, Goldilocks n = 24 went from
+// 2.18 ms (loads interleaved with folds, 3 blocks/SM) to 2.01 ms.
+#ifndef SC_EARLY_LOADS
+#define SC_EARLY_LOADS 1
+#endif
 #ifndef SC_PAIR_UNROLL
 #define SC_PAIR_UNROLL 1
 #endif
@@ -284,6 +290,50 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
 #pragma unroll(SHAPE == kShapeGeneric ? 1 : kPairUnroll)
   for (uint64_t q = first; q < last; q += stride) {
     Fe<L> sh_v[NR], sh_d[NR];
+#if SC_EARLY_LOADS
+    if constexpr (SHAPE != kShapeGeneric && L <= 2) {
+      // every load of the pair first (one 16- or 8-byte load per table and limb plane), then
+      // the folds: the loads of a pair are all in flight together
+      if (fold) {
+        uint4 raw[NR][L];
+#pragma unroll
+        for (int i = 0; i < NR; ++i)
+#pragma unroll
+          for (int l = 0; l < L; ++l)
+            raw[i][l] = __ldcs(reinterpret_cast<const uint4*>(src + (static_cast<uint64_t>(E.role[i]) * L + l) * src_len) + q);
+        const uint64_t dst_len = src_len >> 1;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+          Fe<L> x0, x1, x2, x3;
+#pragma unroll
+          for (int l = 0; l < L; ++l) {
+            x0.w[l] = raw[i][l].x; x1.w[l] = raw[i][l].y; x2.w[l] = raw[i][l].z; x3.w[l] = raw[i][l].w;
+          }
+          const Fe<L> e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
+          const Fe<L> o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
+#pragma unroll
+          for (int l = 0; l < L; ++l)
+            reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(E.role[i]) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+          sh_v[i] = e;
+          sh_d[i] = o;
+        }
+      } else {
+        uint2 raw[NR][L];
+#pragma unroll
+        for (int i = 0; i < NR; ++i)
+#pragma unroll
+          for (int l = 0; l < L; ++l)
+            raw[i][l] = __ldcs(reinterpret_cast<const uint2*>(src + (static_cast<uint64_t>(E.role[i]) * L + l) * src_len) + q);
+#pragma unroll
+        for (int i = 0; i < NR; ++i)
+#pragma unroll
+          for (int l = 0; l < L; ++l) {
+            sh_v[i].w[l] = raw[i][l].x;
+            sh_d[i].w[l] = raw[i][l].y;
+          }
+      }
+    } else
+#endif
 #pragma unroll (SHAPE == kShapeGeneric ? 1 : NR)
     for (int i = 0; i < nv; ++i) {
       const int k = SHAPE == kShapeGeneric ? i : E.role[i];
@@ -519,7 +569,7 @@ constexpr int kPointParallelThreads = 128;
 #endif
 __host__ __device__ constexpr int kernel_min_blocks(int L) { return L >= 8 ? SC_L8_MIN_BLOCKS : 1; }
 #ifndef SC_SHAPE_MIN_BLOCKS
-#define SC_SHAPE_MIN_BLOCKS 3
+#define SC_SHAPE_MIN_BLOCKS 2
 #endif
 // Shape kernels of the 1- and 2-limb fields are memory-bound: ask for more resident blocks.
 __host__ __device__ constexpr int round_min_blocks(int L, int shape) {
