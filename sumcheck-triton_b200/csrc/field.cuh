@@ -26,7 +26,7 @@ namespace sc {
 constexpr int kMaxLimbs = 8;
 constexpr int kMaxPoints = 8;  // t = 0..7, degree <= 7
 
-enum FieldKind : int { kFieldGeneric = 0, kFieldGoldilocks = 1 };
+enum FieldKind : int { kFieldGeneric = 0, kFieldGoldilocks = 1, kFieldMersenne127 = 2 };
 
 template <int L>
 struct Fe {
@@ -144,11 +144,72 @@ __device__ __noinline__ Fe<L> cios_mul_call(const Fe<L> a, const Fe<L> b, const 
   return r;
 }
 
+// Montgomery product for p = 2^127 - 1 and R = 2^128 (x, y < p): R = 2 (mod p), so
+// x y R^-1 = (x y mod p) 2^126, and multiplying a 127-bit residue by 2^126 = 2^-1 is a
+// rotation right by one bit. x y < 2^254 = h 2^127 + l reduces to h + l < 2^128, then
+// (s mod 2^127) + (s >> 127) <= p, then one conditional subtraction of p.
+__device__ __forceinline__ void m127_mul(uint32_t (&r)[4], const uint32_t (&x)[4], const uint32_t (&y)[4]) {
+  uint32_t t[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) t[i] = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint64_t uv = static_cast<uint64_t>(x[j]) * y[i] + t[i + j] + c;
+      t[i + j] = static_cast<uint32_t>(uv);
+      c = uv >> 32;
+    }
+    t[i + 4] = static_cast<uint32_t>(c);
+  }
+  // l = t mod 2^127, h = t >> 127 (both < 2^127); s = l + h
+  uint32_t h[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = (t[i + 3] >> 31) | (t[i + 4] << 1);
+  t[3] &= 0x7fffffffu;
+  uint32_t sw[4];
+  uint64_t c = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t v = static_cast<uint64_t>(t[i]) + h[i] + c;
+    sw[i] = static_cast<uint32_t>(v);
+    c = v >> 32;
+  }
+  // s < 2^128: fold bit 127 back in (2^127 = 1)
+  const uint32_t top = sw[3] >> 31;
+  sw[3] &= 0x7fffffffu;
+  c = top;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t v = static_cast<uint64_t>(sw[i]) + c;
+    sw[i] = static_cast<uint32_t>(v);
+    c = v >> 32;
+  }
+  // now s <= p; s == p means 0
+  const bool is_p = sw[0] == 0xffffffffu && sw[1] == 0xffffffffu && sw[2] == 0xffffffffu && sw[3] == 0x7fffffffu;
+  if (is_p) sw[0] = sw[1] = sw[2] = sw[3] = 0;
+  // times 2^126 = 2^-1: rotate the 127-bit value right by one
+  const uint32_t low = sw[0] & 1u;
+  r[0] = (sw[0] >> 1) | (sw[1] << 31);
+  r[1] = (sw[1] >> 1) | (sw[2] << 31);
+  r[2] = (sw[2] >> 1) | (sw[3] << 31);
+  r[3] = (sw[3] >> 1) | (low << 30);
+}
+
+static __device__ __noinline__ Fe<4> m127_mul_call(const Fe<4> a, const Fe<4> b) {
+  Fe<4> r;
+  m127_mul(r.w, a.w, b.w);
+  return r;
+}
+
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
   if constexpr (K == kFieldGoldilocks && L == 2) {
     gold_mul(r.w, a.w, b.w);
+  } else if constexpr (K == kFieldMersenne127 && L == 4) {
+    r = m127_mul_call(a, b);
   } else if constexpr (L == 1) {
     ptx_mont_mul<1>(r.w, a.w, b.w, F.p, F.np);
   } else if constexpr (L >= SC_OUTLINE_MIN_LIMBS && K == kFieldGeneric) {

@@ -144,7 +144,10 @@ inline int timing_collect(sc_ctx* ctx) {
 inline int degree_class(int d) { return d <= 2 ? 2 : (d <= 4 ? 4 : 7); }
 
 inline int field_kind(const uint32_t* p, int L) {
-  return (L == 2 && p[0] == 1u && p[1] == 0xFFFFFFFFu) ? kFieldGoldilocks : kFieldGeneric;
+  if (L == 2 && p[0] == 1u && p[1] == 0xFFFFFFFFu) return kFieldGoldilocks;
+  if (L == 4 && p[0] == 0xFFFFFFFFu && p[1] == 0xFFFFFFFFu && p[2] == 0xFFFFFFFFu && p[3] == 0x7FFFFFFFu)
+    return kFieldMersenne127;
+  return kFieldGeneric;
 }
 
 // Calls Fn<L, K, DMAX>::run(args...) for the runtime (L, K, DMAX class).
@@ -164,7 +167,9 @@ inline int dispatch(int L, int K, int dclass, Args&&... args) {
     case 2:
       return K == kFieldGoldilocks ? dispatch_degree<Fn, 2, kFieldGoldilocks>(dclass, args...)
                                    : dispatch_degree<Fn, 2, kFieldGeneric>(dclass, args...);
-    case 4: return dispatch_degree<Fn, 4, kFieldGeneric>(dclass, args...);
+    case 4:
+      return K == kFieldMersenne127 ? dispatch_degree<Fn, 4, kFieldMersenne127>(dclass, args...)
+                                    : dispatch_degree<Fn, 4, kFieldGeneric>(dclass, args...);
     default: return dispatch_degree<Fn, 8, kFieldGeneric>(dclass, args...);
   }
 }
@@ -172,7 +177,8 @@ inline int dispatch(int L, int K, int dclass, Args&&... args) {
 // Calls Fn for every instantiation (set-up of kernel attributes).
 template <template <int, int, int> class Fn>
 inline int for_each_instance() {
-  const int combos[5][2] = {{1, kFieldGeneric}, {2, kFieldGeneric}, {2, kFieldGoldilocks}, {4, kFieldGeneric}, {8, kFieldGeneric}};
+  const int combos[6][2] = {{1, kFieldGeneric}, {2, kFieldGeneric}, {2, kFieldGoldilocks},
+                            {4, kFieldGeneric}, {4, kFieldMersenne127}, {8, kFieldGeneric}};
   for (const auto& c : combos)
     for (int dc : {2, 4, 7}) {
       const int rc = dispatch<Fn>(c[0], c[1], dc);
@@ -227,7 +233,9 @@ inline bool cios_bound_holds(const HostField& hf) {
 }
 
 // Instruction-count estimates of one product and one modular add (for the choices below).
-inline int mul_cost(int L, int K) { return K == kFieldGoldilocks ? 16 : (L == 1 ? 10 : 4 * L * L + 8 * L); }
+inline int mul_cost(int L, int K) {
+  return K == kFieldGoldilocks ? 16 : (K == kFieldMersenne127 ? 60 : (L == 1 ? 10 : 4 * L * L + 8 * L));
+}
 inline int add_cost(int L) { return 3 * L + 4; }
 
 // Whether a term of length len in an expression of degree d is cheaper evaluated at points
