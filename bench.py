@@ -478,6 +478,9 @@ def main() -> int:
             roof["traffic_source"] = (f"dram__bytes_read.sum + dram__bytes_write.sum of every {L}-limb tick of the "
                                       f"64-proof cut (profiles/), {ratio:.3f} x the algorithmic bytes, applied to "
                                       f"this run's algorithmic bytes per launch")
+        if path == "batched" and len(per_class) > 1:
+            roof["note"] = ("the field groups run concurrently on their own streams; a class's launch "
+                            "durations include the other group's use of the SMs")
         roof["by_class"] = {f"L{k}": {"busy_ms": v["ms"], "launches": v["launches"],
                                       "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                       "TIMAD/s": v["imad"] / (v["ms"] / 1e3) / 1e12} for k, v in per_class.items()}

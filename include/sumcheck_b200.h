@@ -194,6 +194,12 @@ int sc_batch_create_tiled(sc_ctx* ctx, const sc_field* field, int count, const s
 /* Enqueues one run after the work queued on the context's stream (the context's stream
  * then waits for it). Asynchronous. */
 int sc_batch_run(sc_batch* batch);
+/* sc_batch_run in two halves, so that batches sharing a context overlap on the device:
+ * sc_batch_launch enqueues the run after the work queued on the context's stream and returns;
+ * sc_batch_join makes the context's stream wait for that run. Launch every batch, then join
+ * every batch. */
+int sc_batch_launch(sc_batch* batch);
+int sc_batch_join(sc_batch* batch);
 /* Waits for the last run; its results are then readable with sc_batch_result. */
 int sc_batch_wait(sc_batch* batch);
 /* Outputs of proof `index` of the last run, laid out as sc_prove's. */

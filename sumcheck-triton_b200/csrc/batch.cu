@@ -357,7 +357,7 @@ int sc_batch_create(sc_ctx* ctx, const sc_field* field, int count, const sc_expr
   return sc_batch_create_tiled(ctx, field, count, exprs, num_rounds, tables_dev, challenge_mode, ct, ppt.data(), out);
 }
 
-int sc_batch_run(sc_batch* B) {
+int sc_batch_launch(sc_batch* B) {
   if (!B) return fail(SC_ERR_INVALID, "NULL batch");
   SC_CUDA(cudaSetDevice(B->ctx->device));
   // the batch starts after the work already queued on the caller's stream
@@ -379,8 +379,19 @@ int sc_batch_run(sc_batch* B) {
   }
   SC_CUDA(cudaGraphLaunch(B->exec, B->stream));
   SC_CUDA(cudaEventRecord(B->done, B->stream));
+  return SC_OK;
+}
+
+int sc_batch_join(sc_batch* B) {
+  if (!B) return fail(SC_ERR_INVALID, "NULL batch");
+  SC_CUDA(cudaSetDevice(B->ctx->device));
   SC_CUDA(cudaStreamWaitEvent(B->ctx->stream, B->done, 0));
   return SC_OK;
+}
+
+int sc_batch_run(sc_batch* B) {
+  const int rc = sc_batch_launch(B);
+  return rc ? rc : sc_batch_join(B);
 }
 
 int sc_batch_wait(sc_batch* B) {

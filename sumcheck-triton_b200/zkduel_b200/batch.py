@@ -95,10 +95,13 @@ class BatchProver:
             self._keep.append((expr_arr, rounds, tabs))
 
     def launch(self) -> None:
-        """Enqueues one run of every group (asynchronous)."""
+        """Enqueues one run of every group (asynchronous). Every group is launched before any
+        is joined to the caller's stream, so the groups run concurrently on their own streams."""
         lib = _lib.load()
         for g in self.groups:
-            _lib.check(lib.sc_batch_run(g.handle), "sc_batch_run")
+            _lib.check(lib.sc_batch_launch(g.handle), "sc_batch_launch")
+        for g in self.groups:
+            _lib.check(lib.sc_batch_join(g.handle), "sc_batch_join")
 
     def wait(self) -> None:
         lib = _lib.load()
