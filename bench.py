@@ -640,13 +640,29 @@ def e2e_measure(work: Workload, args, device, batcher=None) -> dict:
     lib = _lib.load()
 
     if batcher is not None:
+        # the copies spread over E2E_COPY_STREAMS streams (each with its own context for the
+        # conversion), joined into the proving stream before the batch runs
+        nstreams = int(os.environ.get("E2E_COPY_STREAMS", "3"))
+        streams = [torch.cuda.Stream(device) for _ in range(nstreams)]
+        ctxs = []
+        for st in streams:
+            with torch.cuda.stream(st):
+                ctxs.append(api.get_context(device))
+
         def step():
-            for (s, spec, _e, t), h in zip(work.items, host):
-                t.copy_(h, non_blocking=True)
+            main = torch.cuda.current_stream(device)
+            for st in streams:
+                st.wait_stream(main)
+            for i, ((s, spec, _e, t), h) in enumerate(zip(work.items, host)):
+                st, c = streams[i % nstreams], ctxs[i % nstreams]
+                with torch.cuda.stream(st):
+                    t.copy_(h, non_blocking=True)
                 fld = api.get_device_field(spec, ctx.device)
                 K, _L, N = t.shape
-                _lib.check(lib.sc_tables_to_mont(ctx.handle, fld.handle, ctypes.c_void_p(t.data_ptr()),
+                _lib.check(lib.sc_tables_to_mont(c.handle, fld.handle, ctypes.c_void_p(t.data_ptr()),
                                                  ctypes.c_uint64(N), int(K)), "sc_tables_to_mont")
+            for st in streams:
+                main.wait_stream(st)
             batcher.run()
             return batcher.results()
     else:
