@@ -220,6 +220,33 @@ int sc_batch_tick_times(sc_batch* batch, float* out_start_ms, float* out_end_ms,
                         int* count);
 int sc_batch_destroy(sc_batch* batch);
 
+/* ---- One proof split across ranks ----------------------------------------------------
+ * Replaces: nothing; the reference proves on one device (cuda/src/field_sumcheck.cu:1012-1088).
+ *
+ * With world = 2^w ranks, rank r holds entries [r C, (r + 1) C), C = 2^(num_rounds - w), of
+ * every table (limb-planar, C entries per plane). Protocol, identical on every rank:
+ *   for j in 0 .. sc_split_local_rounds() - 1:
+ *     sc_split_round(j, share)            this rank's share of g_j(0..d): (d + 1) L words
+ *     all-gather the shares (rank order)  (the caller's collective, e.g. NCCL)
+ *     sc_split_commit(j, shares)          sum, checksum, SHA3 challenge, claim (on the device)
+ *   sc_split_last_entries(entries)        this rank's chunk folded to one entry per table (K L)
+ *   all-gather the entries (rank order)
+ *   sc_split_finish(all_entries)          the last w rounds on the W-entry tables
+ *   sc_split_result(...)                  as sc_prove's outputs; the same on every rank and
+ *                                         bit-identical to sc_prove on the whole tables.
+ * With world = 1 the protocol is a whole proof (sc_split_finish(NULL)). */
+typedef struct sc_split sc_split;
+int sc_split_create(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds, int world,
+                    int rank, const uint32_t* local_tables_dev, int challenge_mode, sc_split** out);
+int sc_split_local_rounds(const sc_split* split);
+int sc_split_round(sc_split* split, int round, uint32_t* out_share);
+int sc_split_commit(sc_split* split, int round, const uint32_t* shares);
+int sc_split_last_entries(sc_split* split, uint32_t* out_entries);
+int sc_split_finish(sc_split* split, const uint32_t* all_entries);
+int sc_split_result(sc_split* split, uint32_t* out_round_polys, uint32_t* out_challenges,
+                    uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum);
+int sc_split_destroy(sc_split* split);
+
 /* ---- Served proving -------------------------------------------------------------------
  * Replaces: nothing in the reference runs more than one proof at a time; its callers loop
  * over proofs (cuda/src/field_sumcheck.cu:1178-1336, src/zkduel/api.py:26-64).

@@ -21,7 +21,7 @@ OBJ = Path(os.environ.get("SC_BUILD_DIR", PKG / "_build"))
 CLI = PKG / "bin" / "field_sumcheck_b200"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
-SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "serve.cu"]
+SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "serve.cu", "split.cu"]
 
 
 def _stale(target: Path, deps) -> bool:

@@ -78,6 +78,7 @@ struct ProveRun {
                               ctx->stream));
 
     RoundArgs A;
+    std::memset(&A, 0, sizeof(A));
     A.num_rounds = n;
     A.mode = mode;
     A.partials = static_cast<uint32_t*>(ctx->partials.p);

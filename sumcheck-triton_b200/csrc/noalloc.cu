@@ -107,6 +107,7 @@ static int run(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const u
                             ctx->stream));
 
   RoundArgs A;
+  std::memset(&A, 0, sizeof(A));
   A.num_rounds = n;
   A.mode = mode;
   A.partials = base + w_part;

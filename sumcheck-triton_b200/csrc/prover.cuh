@@ -113,6 +113,8 @@ struct RoundArgs {
   uint32_t* partials;    // [gridDim.x][kMaxPoints][L]
   const FieldConsts* fc;
   ProofState st;
+  uint32_t* ext_out;     // non-null: the round's sums g_j(0..d) go here and the round is not
+                         // finalised (one rank of a split proof; the commit finalises it)
 };
 
 template <int L>
@@ -610,7 +612,11 @@ __global__ void __launch_bounds__(kernel_threads(L), round_min_blocks(L, SHAPE))
   if (!is_last) return;
   __threadfence();
   reduce_partials<L, K, DMAX + 1>(A.partials, 0, gridDim.x, d, smem, g_sm, F);
-  if (tid < 32) finalize_round<L, K>(A, E, F, g_sm, msg);
+  if (A.ext_out) {
+    for (int i = tid; i < (d + 1) * L; i += nthr) A.ext_out[i] = g_sm[i];
+  } else if (tid < 32) {
+    finalize_round<L, K>(A, E, F, g_sm, msg);
+  }
   if (tid == 0) {
     __threadfence();
     *A.st.counter = 0;

@@ -247,7 +247,11 @@ __global__ void __launch_bounds__(128, 4) round_kernel_pp(const RoundArgs A, con
   if (!is_last) return;
   __threadfence();
   pp_reduce_partials<L, K>(A.partials, gridDim.x, d, smem, g_sm, F);
-  if (tid < 32) finalize_round<L, K>(A, E, F, g_sm, msg);
+  if (A.ext_out) {
+    for (int i = tid; i < (d + 1) * L; i += blockDim.x) A.ext_out[i] = g_sm[i];
+  } else if (tid < 32) {
+    finalize_round<L, K>(A, E, F, g_sm, msg);
+  }
   if (tid == 0) {
     __threadfence();
     *A.st.counter = 0;

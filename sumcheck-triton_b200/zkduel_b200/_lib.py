@@ -99,6 +99,14 @@ SIGNATURES = {
     "sc_batch_class_proofs": (c_int, [c_void_p, c_int, POINTER(c_int32), c_int, POINTER(c_int)]),
     "sc_batch_destroy": (c_int, [c_void_p]),
     "sc_calibrate_imad": (c_int, [c_void_p, POINTER(c_double)]),
+    "sc_split_create": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, POINTER(c_void_p)]),
+    "sc_split_local_rounds": (c_int, [c_void_p]),
+    "sc_split_round": (c_int, [c_void_p, c_int, U32P]),
+    "sc_split_commit": (c_int, [c_void_p, c_int, U32P]),
+    "sc_split_last_entries": (c_int, [c_void_p, U32P]),
+    "sc_split_finish": (c_int, [c_void_p, U32P]),
+    "sc_split_result": (c_int, [c_void_p, U32P, U32P, U32P, U32P, U64P]),
+    "sc_split_destroy": (c_int, [c_void_p]),
     "sc_server_create": (
         c_int, [c_int, c_void_p, c_int, c_uint64, c_int, c_int, c_int, c_int, c_int, POINTER(c_void_p)],
     ),
