@@ -37,6 +37,7 @@ extern "C" {
 #define SC_ERR_NOMEM 6          /* device or host allocation failed                     */
 #define SC_ERR_TIMEOUT 7        /* a bounded wait ran out (sc_server_wait / _drain)     */
 #define SC_ERR_PENDING 8        /* the request has not completed yet                    */
+#define SC_SUSPENDED 9          /* the request was suspended; its transcript is readable */
 
 #define SC_CHALLENGE_SHA3 0     /* r_j = SHA3 transcript rule (field_sumcheck.cu:857-907) */
 #define SC_CHALLENGE_FIXED 1    /* r_j = 1 (field_sumcheck.cu:1058)                       */
@@ -247,6 +248,51 @@ int sc_split_result(sc_split* split, uint32_t* out_round_polys, uint32_t* out_ch
                     uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum);
 int sc_split_destroy(sc_split* split);
 
+/* ---- Transcripts: suspending and resuming a proof ----------------------------------
+ * No counterpart in the reference: its proofs run start to finish inside one call.
+ *
+ * A transcript is a proof stopped at a round boundary: a flat array of u32 words that a
+ * caller may store anywhere (file, database, another process) and later continue from the
+ * same tables, on any context or server of the same field, with results bit-identical to
+ * the uninterrupted proof. Layout (little-endian words):
+ *   0  magic 0x31524353 ("SCR1")     1  header words (16)    2  limbs L
+ *   3  num_rounds n                  4  num_vars K            5  degree d
+ *   6  challenge mode                7  rounds done j (0..n)
+ *   8  expression digest (u64)      10  field digest (u64)   12  tables tag (u64)
+ *  14  state words S                15  0
+ *  16  state: [0] 0, [1] device status, [2..3] checksum so far (u64), then
+ *      g_0..g_{n-1}   n x 8 x L     (slot t of round i: g_i(t); rounds < j filled)
+ *      r_0..r_{n-1}   n x L
+ *      finals         (1 + K) x L   (when j = n)
+ *      claim0         L
+ *      claim          L             (g_{j-1}(r_{j-1}), the claim round j meets)
+ * S = 4 + L (9 n + K + 3); sc_transcript_words() = 16 + S.
+ * The digests bind a transcript to its field and expression; the tables tag is the
+ * caller's name for the tables (sc_tables_tag for seeded ones; any value otherwise) and
+ * is carried, not checked, by sc_prove_resume. Resuming folds the tables up to round j
+ * with the recorded challenges (about one pass over them), then proves on. */
+int sc_transcript_words(const sc_field* field, const sc_expr* expr, int num_rounds, uint64_t* out_words);
+/* A transcript with no rounds done (the caller's `words`-word array). */
+int sc_transcript_init(const sc_field* field, const sc_expr* expr, int num_rounds, int challenge_mode,
+                       uint64_t tables_tag, uint32_t* transcript, uint64_t words);
+/* Header of a transcript (checked for consistency); any output may be NULL. Host only. */
+int sc_transcript_info(const uint32_t* transcript, uint64_t words, int* out_num_rounds,
+                       int* out_rounds_done, int* out_challenge_mode, uint64_t* out_tables_tag);
+/* Outputs of a complete transcript, laid out as sc_prove's; SC_ERR_PENDING before that. */
+int sc_transcript_result(const sc_field* field, const sc_expr* expr, const uint32_t* transcript,
+                         uint64_t words, uint32_t* out_round_polys, uint32_t* out_challenges,
+                         uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum);
+/* The tag of tables generated by sc_tables_generate(num_tables, table_kinds, seed): what
+ * the server records in its requests' transcripts and checks on resume. Host only. */
+int sc_tables_tag(int num_tables, const int32_t* table_kinds, uint64_t seed, uint64_t* out_tag);
+/* Proves rounds [rounds done, stop_round) of the transcript's proof on tables_dev (T_0,
+ * as for sc_prove) and updates the transcript in place; stop_round = num_rounds completes
+ * it. Explicit mode: explicit_challenges holds all num_rounds challenges, and the ones
+ * already used must equal the transcript's. Synchronous, like sc_prove. */
+int sc_prove_resume(sc_ctx* ctx, const sc_field* field, const sc_expr* expr,
+                    const uint32_t* tables_dev, const uint32_t* explicit_challenges, int stop_round,
+                    uint32_t* transcript, uint64_t words);
+
 /* ---- Served proving -------------------------------------------------------------------
  * Replaces: nothing in the reference runs more than one proof at a time; its callers loop
  * over proofs (cuda/src/field_sumcheck.cu:1178-1336, src/zkduel/api.py:26-64).
@@ -278,7 +324,7 @@ typedef struct sc_server sc_server;
 #define SC_SERVE_FIFO_PLAIN 1
 
 typedef struct sc_server_stats {
-  uint64_t submitted, completed, failed;
+  uint64_t submitted, completed, failed, suspended;
   uint64_t ticks;              /* launches groups issued (continuous policy) */
   uint64_t items;              /* (request, tile) items issued */
   uint64_t peak_inflight;      /* most requests admitted at once */
@@ -322,6 +368,22 @@ int sc_server_times(sc_server* server, uint64_t id, double* out_submit_s, double
                     double* out_done_s);
 /* Forgets a completed request (its result is no longer readable). */
 int sc_server_release(sc_server* server, uint64_t id);
+/* Suspends request `id` (0: every request not finished) at its next round boundary: its
+ * device memory goes back to the pool and its transcript is kept; sc_server_wait then
+ * returns SC_SUSPENDED. Queued requests are suspended where they stand (rounds done as
+ * submitted). Requests that finish first, and large requests already issued whole on
+ * the lane, complete normally. Thread-safe; returns at once. */
+int sc_server_suspend(sc_server* server, uint64_t id);
+/* Transcript of a suspended request (sc_transcript_words words; carries the tag of its
+ * seeded tables). */
+int sc_server_transcript(sc_server* server, uint64_t id, uint32_t* transcript, uint64_t words);
+/* Queues a request that continues the transcript's proof: the same expression, rounds,
+ * table kinds and seed as the transcript's tables (the tag is checked), its challenge mode
+ * (SHA3 or fixed). The tables are generated from the seed again and folded to the
+ * transcript's round at admission; results are bit-identical to the uninterrupted proof. */
+int sc_server_submit_resume(sc_server* server, const sc_expr* expr, const int32_t* table_kinds,
+                            uint64_t seed, const uint32_t* transcript, uint64_t words,
+                            uint64_t* out_id);
 int sc_server_stats_get(sc_server* server, sc_server_stats* out);
 /* Stops accepting requests, finishes the queued ones, joins the worker, frees everything. */
 int sc_server_destroy(sc_server* server);

@@ -22,10 +22,12 @@ inline bool round_skip1(int n, int j) { return j >= 1 && (uint64_t{1} << (n - j 
 
 template <int L, int K, int DMAX>
 struct ProveRun {
+  // Rounds [first, stop) of the proof. state_io (host, state words; NULL for a whole proof
+  // from round 0): the state after round first - 1 in, the state after round stop - 1 out.
   static int run(sc_ctx* ctx, const sc_field* f, const sc_expr* ex, int n, const uint32_t* tables, int mode,
                  const uint32_t* explicit_ch, uint32_t* out_polys, uint32_t* out_ch, uint32_t* out_finals,
-                 uint32_t* out_claim0, uint64_t* out_checksum) {
-    const int K_ = ex->num_vars, d = ex->degree;
+                 uint32_t* out_claim0, uint64_t* out_checksum, int first, int stop, uint32_t* state_io) {
+    const int K_ = ex->num_vars;
     const uint64_t N = uint64_t{1} << n;
     // scratch
     const size_t fold_a_words = n >= 2 ? static_cast<size_t>(K_) * L * (N / 2) : 0;
@@ -72,7 +74,10 @@ struct ProveRun {
     F.np = f->hf.np;
 
     uint32_t* st = static_cast<uint32_t*>(ctx->state.p);
-    SC_CUDA(cudaMemsetAsync(st, 0, so.total_words * 4, ctx->stream));
+    if (state_io)
+      SC_CUDA(cudaMemcpyAsync(st, state_io, so.total_words * 4, cudaMemcpyHostToDevice, ctx->stream));
+    else
+      SC_CUDA(cudaMemsetAsync(st, 0, so.total_words * 4, ctx->stream));
     if (mode == SC_CHALLENGE_EXPLICIT)
       SC_CUDA(cudaMemcpyAsync(st + so.chals, explicit_ch, static_cast<size_t>(n) * L * 4, cudaMemcpyHostToDevice,
                               ctx->stream));
@@ -92,8 +97,12 @@ struct ProveRun {
     A.st.claim0 = st + so.claim0;
     A.st.claim = st + so.claim;
 
-    const uint32_t* prev = tables;  // T_{j-1} (or T_0)
-    for (int j = 0; j < n; ++j) {
+    // T_{first-1} (or T_0), refolded from T_0 with the recorded challenges when resuming
+    if ((rc = resume_folds(f, n, K_, tables, static_cast<uint32_t*>(ctx->fold_a.p), static_cast<uint32_t*>(ctx->fold_b.p),
+                           st + so.chals, first, ctx->sm_count, ctx->stream)))
+      return rc;
+    const uint32_t* prev = first <= 1 ? tables : static_cast<const uint32_t*>(((first - 1) & 1) ? ctx->fold_a.p : ctx->fold_b.p);
+    for (int j = first; j < stop; ++j) {
       A.round = j;
       A.pairs = N >> (j + 1);
       A.skip1 = round_skip1(n, j) ? 1 : 0;
@@ -124,7 +133,16 @@ struct ProveRun {
       SC_CUDA(cudaGetLastError());
       if ((rc = timing_end(ctx))) return rc;
     }
-    // results
+    return finish(ctx, ex, n, stop, st, so, out_polys, out_ch, out_finals, out_claim0, out_checksum, state_io);
+  }
+
+  // One copy of the state to pinned memory, then the caller's arrays (outputs only when the
+  // proof is complete) and the state words.
+  static int finish(sc_ctx* ctx, const sc_expr* ex, int n, int stop, const uint32_t* st, const StateOffsets& so,
+                    uint32_t* out_polys, uint32_t* out_ch, uint32_t* out_finals, uint32_t* out_claim0,
+                    uint64_t* out_checksum, uint32_t* state_io) {
+    const int d = ex->degree, K_ = ex->num_vars;
+    int rc;
     if (ctx->host_state_bytes < so.total_words * 4) {
       if (ctx->host_state) cudaFreeHost(ctx->host_state);
       ctx->host_state = nullptr;
@@ -137,6 +155,8 @@ struct ProveRun {
     if ((rc = timing_collect(ctx))) return rc;
     const uint32_t* hs = ctx->host_state;
     if (hs[so.status]) return fail(SC_ERR_DEVICE, "device status %u", hs[so.status]);
+    if (state_io) std::memcpy(state_io, hs, so.total_words * 4);
+    if (stop < n) return SC_OK;
     if (out_polys)
       for (int j = 0; j < n; ++j)
         std::memcpy(out_polys + static_cast<size_t>(j) * (d + 1) * L, hs + so.polys + static_cast<size_t>(j) * kMaxPoints * L,
@@ -148,6 +168,27 @@ struct ProveRun {
     return SC_OK;
   }
 };
+
+template <int L, int K>
+int fold_prefix(const sc_field* f, int n, int num_tables, const uint32_t* tables, uint32_t* fold_a, uint32_t* fold_b,
+                const uint32_t* chals_dev, int j, int sm_count, cudaStream_t stream) {
+  FieldParams<L, K> F;
+  for (int l = 0; l < L; ++l) F.p[l] = f->hf.p[l];
+  F.np = f->hf.np;
+  const uint64_t N = uint64_t{1} << n;
+  const uint32_t* src = tables;
+  for (int i = 1; i < j; ++i) {
+    uint32_t* dst = (i & 1) ? fold_a : fold_b;
+    const uint64_t src_len = N >> (i - 1);
+    const uint64_t total = (src_len >> 2) * static_cast<uint64_t>(num_tables);
+    const unsigned grid = static_cast<unsigned>(
+        std::max<uint64_t>(1, std::min<uint64_t>((total + 255) / 256, static_cast<uint64_t>(sm_count) * 8)));
+    fold_kernel<L, K><<<grid, 256, 0, stream>>>(src, dst, src_len, num_tables, chals_dev + static_cast<size_t>(i - 1) * L, F);
+    SC_CUDA(cudaGetLastError());
+    src = dst;
+  }
+  return SC_OK;
+}
 
 template <int L>
 int generate_impl(sc_ctx* ctx, const sc_field* f, int num_tables, int n, const int32_t* kinds,
@@ -512,7 +553,135 @@ int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_ro
   SC_CUDA(cudaSetDevice(ctx->device));
   return dispatch<ProveRun>(field->hf.L, field_kind(field->hf.p, field->hf.L), degree_class(expr->degree), ctx, field,
                             expr, num_rounds, tables_dev, challenge_mode, explicit_challenges, out_round_polys,
-                            out_challenges, out_finals, out_claim0, out_checksum);
+                            out_challenges, out_finals, out_claim0, out_checksum, 0, num_rounds, nullptr);
+}
+
+}  // extern "C"
+
+namespace sc_host {
+
+int resume_folds(const sc_field* f, int n, int num_tables, const uint32_t* tables, uint32_t* fold_a, uint32_t* fold_b,
+                 const uint32_t* chals_dev, int j, int sm_count, cudaStream_t stream) {
+  if (j <= 1) return SC_OK;
+  if (j > n - 1) return fail(SC_ERR_INVALID, "resume at round %d of %d", j, n);
+  const int L = f->hf.L;
+  switch (L) {
+    case 1: return fold_prefix<1, kFieldGeneric>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream);
+    case 2:
+      return field_kind(f->hf.p, L) == kFieldGoldilocks
+                 ? fold_prefix<2, kFieldGoldilocks>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream)
+                 : fold_prefix<2, kFieldGeneric>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream);
+    case 4:
+      return field_kind(f->hf.p, L) == kFieldMersenne127
+                 ? fold_prefix<4, kFieldMersenne127>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream)
+                 : fold_prefix<4, kFieldGeneric>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream);
+    default: return fold_prefix<8, kFieldGeneric>(f, n, num_tables, tables, fold_a, fold_b, chals_dev, j, sm_count, stream);
+  }
+}
+
+int prove_segment(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int n, const uint32_t* tables, int mode,
+                  const uint32_t* explicit_ch, int first, int stop, uint32_t* state_io) {
+  if (first < 0 || stop <= first || stop > n) return fail(SC_ERR_INVALID, "rounds [%d, %d) of %d", first, stop, n);
+  SC_CUDA(cudaSetDevice(ctx->device));
+  return dispatch<ProveRun>(field->hf.L, field_kind(field->hf.p, field->hf.L), degree_class(expr->degree), ctx, field,
+                            expr, n, tables, mode, explicit_ch, nullptr, nullptr, nullptr, nullptr, nullptr, first, stop,
+                            state_io);
+}
+
+}  // namespace sc_host
+
+extern "C" {
+
+int sc_transcript_words(const sc_field* field, const sc_expr* expr, int num_rounds, uint64_t* out_words) {
+  if (!field || !expr || !out_words) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_rounds < 1 || num_rounds > kMaxRounds)
+    return fail(SC_ERR_INVALID, "num_rounds %d outside 1..%d", num_rounds, kMaxRounds);
+  *out_words = transcript_words(num_rounds, expr->num_vars, field->hf.L);
+  return SC_OK;
+}
+
+int sc_transcript_init(const sc_field* field, const sc_expr* expr, int num_rounds, int challenge_mode,
+                       uint64_t tables_tag, uint32_t* transcript, uint64_t words) {
+  uint64_t need = 0;
+  int rc = sc_transcript_words(field, expr, num_rounds, &need);
+  if (rc) return rc;
+  if (!transcript) return fail(SC_ERR_INVALID, "NULL transcript");
+  if (challenge_mode < SC_CHALLENGE_SHA3 || challenge_mode > SC_CHALLENGE_EXPLICIT)
+    return fail(SC_ERR_INVALID, "unknown challenge mode %d", challenge_mode);
+  if (words < need) return fail(SC_ERR_INVALID, "transcript needs %llu words, got %llu",
+                                static_cast<unsigned long long>(need), static_cast<unsigned long long>(words));
+  std::memset(transcript, 0, need * 4);
+  transcript_header(transcript, field->hf, *expr, num_rounds, challenge_mode, 0, tables_tag);
+  return SC_OK;
+}
+
+int sc_transcript_info(const uint32_t* transcript, uint64_t words, int* out_num_rounds, int* out_rounds_done,
+                       int* out_challenge_mode, uint64_t* out_tables_tag) {
+  TranscriptInfo I;
+  int rc = transcript_parse(transcript, words, &I);
+  if (rc) return rc;
+  if (out_num_rounds) *out_num_rounds = I.n;
+  if (out_rounds_done) *out_rounds_done = I.done;
+  if (out_challenge_mode) *out_challenge_mode = I.mode;
+  if (out_tables_tag) *out_tables_tag = I.tag;
+  return SC_OK;
+}
+
+int sc_transcript_result(const sc_field* field, const sc_expr* expr, const uint32_t* transcript, uint64_t words,
+                         uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
+                         uint32_t* out_claim0, uint64_t* out_checksum) {
+  if (!field || !expr) return fail(SC_ERR_INVALID, "NULL argument");
+  TranscriptInfo I;
+  int rc = transcript_parse(transcript, words, &I);
+  if (!rc) rc = transcript_match(I, field->hf, *expr);
+  if (rc) return rc;
+  if (I.done < I.n) return fail(SC_ERR_PENDING, "transcript has %d of %d rounds", I.done, I.n);
+  const int L = I.L, d = I.d, n = I.n;
+  const StateOffsets so = state_offsets(n, I.K, L);
+  const uint32_t* hs = transcript + kTranscriptHeader;
+  if (out_round_polys)
+    for (int j = 0; j < n; ++j)
+      std::memcpy(out_round_polys + static_cast<size_t>(j) * (d + 1) * L, hs + so.polys + static_cast<size_t>(j) * kMaxPoints * L,
+                  static_cast<size_t>(d + 1) * L * 4);
+  if (out_challenges) std::memcpy(out_challenges, hs + so.chals, static_cast<size_t>(n) * L * 4);
+  if (out_finals) std::memcpy(out_finals, hs + so.finals, static_cast<size_t>(1 + I.K) * L * 4);
+  if (out_claim0) std::memcpy(out_claim0, hs + so.claim0, static_cast<size_t>(L) * 4);
+  if (out_checksum) std::memcpy(out_checksum, hs + so.checksum, 8);
+  return SC_OK;
+}
+
+int sc_tables_tag(int num_tables, const int32_t* table_kinds, uint64_t seed, uint64_t* out_tag) {
+  if (!table_kinds || !out_tag) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_tables < 1 || num_tables > kMaxVars) return fail(SC_ERR_INVALID, "num_tables %d outside 1..%d", num_tables, kMaxVars);
+  *out_tag = seeded_tables_tag(num_tables, table_kinds, seed);
+  return SC_OK;
+}
+
+int sc_prove_resume(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, const uint32_t* tables_dev,
+                    const uint32_t* explicit_challenges, int stop_round, uint32_t* transcript, uint64_t words) {
+  if (!ctx || !field || !expr || !tables_dev) return fail(SC_ERR_INVALID, "NULL argument");
+  TranscriptInfo I;
+  int rc = transcript_parse(transcript, words, &I);
+  if (!rc) rc = transcript_match(I, field->hf, *expr);
+  if (rc) return rc;
+  if (I.done == I.n) return fail(SC_ERR_INVALID, "the transcript's proof is complete");
+  if (stop_round <= I.done || stop_round > I.n)
+    return fail(SC_ERR_INVALID, "stop_round %d outside %d..%d", stop_round, I.done + 1, I.n);
+  if (reinterpret_cast<uintptr_t>(tables_dev) % 16) return fail(SC_ERR_INVALID, "tables_dev must be 16-byte aligned");
+  if (field->device != ctx->device)
+    return fail(SC_ERR_INVALID, "field was set up on device %d, context is on %d", field->device, ctx->device);
+  uint32_t* state = transcript + kTranscriptHeader;
+  const StateOffsets so = state_offsets(I.n, I.K, I.L);
+  if (state[so.counter] || state[so.status]) return fail(SC_ERR_INVALID, "transcript state records a device error");
+  if (I.mode == SC_CHALLENGE_EXPLICIT) {
+    if (!explicit_challenges) return fail(SC_ERR_INVALID, "explicit challenge mode needs explicit_challenges");
+    if (std::memcmp(explicit_challenges, state + so.chals, static_cast<size_t>(I.done) * I.L * 4))
+      return fail(SC_ERR_INVALID, "explicit challenges differ from the transcript's first %d", I.done);
+  }
+  rc = prove_segment(ctx, field, expr, I.n, tables_dev, I.mode, explicit_challenges, I.done, stop_round, state);
+  if (rc) return rc;
+  transcript[kTwDone] = static_cast<uint32_t>(stop_round);
+  return SC_OK;
 }
 
 }  // extern "C"

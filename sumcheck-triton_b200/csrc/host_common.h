@@ -407,4 +407,139 @@ int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int 
 int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
                         cudaStream_t stream, const BatchTickArgs& T);
 
+// ---- transcripts: a proof stopped at a round boundary, resumable from the same tables
+//
+// A transcript is the header below followed by the proof-state words (state_offsets
+// layout) as the round kernels leave them after round rounds_done - 1: checksum so far,
+// g_j for j < rounds_done, r_j for j < rounds_done, claim0, and the claim the next round
+// meets. That is all a later call needs: the challenges refold the tables to the round it
+// continues from, and finalize_round goes on adding to the same checksum.
+constexpr uint32_t kTranscriptMagic = 0x31524353u;  // "SCR1"
+constexpr int kTranscriptHeader = 16;
+enum TranscriptWord {
+  kTwMagic = 0, kTwHeaderWords = 1, kTwLimbs = 2, kTwRounds = 3, kTwVars = 4, kTwDegree = 5, kTwMode = 6,
+  kTwDone = 7, kTwExprDigest = 8, kTwFieldDigest = 10, kTwTablesTag = 12, kTwStateWords = 14,
+};
+
+constexpr uint64_t kFnvBasis = 0xcbf29ce484222325ull;
+
+inline uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
+
+template <typename T>
+inline uint64_t fnv1a_vec(uint64_t h, const std::vector<T>& v) {
+  const uint64_t n = v.size();
+  h = fnv1a(h, &n, sizeof(n));
+  return v.empty() ? h : fnv1a(h, v.data(), v.size() * sizeof(T));
+}
+
+inline uint64_t expr_digest(const sc_expr& e) {
+  const int32_t dims[3] = {e.num_vars, e.num_terms, e.degree};
+  uint64_t h = fnv1a(kFnvBasis, dims, sizeof(dims));
+  h = fnv1a_vec(h, e.coeffs);
+  h = fnv1a_vec(h, e.coeff_limbs);
+  h = fnv1a_vec(h, e.lens);
+  h = fnv1a_vec(h, e.offs);
+  return fnv1a_vec(h, e.flat);
+}
+
+inline uint64_t field_digest(const HostField& hf) {
+  const int32_t L = hf.L;
+  uint64_t h = fnv1a(kFnvBasis, &L, sizeof(L));
+  return fnv1a(h, hf.p, static_cast<size_t>(L) * 4);
+}
+
+// The tag of seeded tables (sc_tables_tag; the server's requests carry it).
+inline uint64_t seeded_tables_tag(int num_tables, const int32_t* kinds, uint64_t seed) {
+  const char dom[] = "sc:seeded-tables:v1";
+  uint64_t h = fnv1a(kFnvBasis, dom, sizeof(dom) - 1);
+  const int32_t k = num_tables;
+  h = fnv1a(h, &k, sizeof(k));
+  h = fnv1a(h, kinds, static_cast<size_t>(num_tables) * 4);
+  return fnv1a(h, &seed, sizeof(seed));
+}
+
+inline size_t transcript_words(int n, int K, int L) {
+  return kTranscriptHeader + state_offsets(n, K, L).total_words;
+}
+
+inline void tw_put64(uint32_t* t, int w, uint64_t v) {
+  t[w] = static_cast<uint32_t>(v);
+  t[w + 1] = static_cast<uint32_t>(v >> 32);
+}
+inline uint64_t tw_get64(const uint32_t* t, int w) { return t[w] | (static_cast<uint64_t>(t[w + 1]) << 32); }
+
+inline void transcript_header(uint32_t* t, const HostField& hf, const sc_expr& ex, int n, int mode, int done,
+                              uint64_t tag) {
+  std::memset(t, 0, kTranscriptHeader * 4);
+  t[kTwMagic] = kTranscriptMagic;
+  t[kTwHeaderWords] = kTranscriptHeader;
+  t[kTwLimbs] = static_cast<uint32_t>(hf.L);
+  t[kTwRounds] = static_cast<uint32_t>(n);
+  t[kTwVars] = static_cast<uint32_t>(ex.num_vars);
+  t[kTwDegree] = static_cast<uint32_t>(ex.degree);
+  t[kTwMode] = static_cast<uint32_t>(mode);
+  t[kTwDone] = static_cast<uint32_t>(done);
+  tw_put64(t, kTwExprDigest, expr_digest(ex));
+  tw_put64(t, kTwFieldDigest, field_digest(hf));
+  tw_put64(t, kTwTablesTag, tag);
+  t[kTwStateWords] = static_cast<uint32_t>(state_offsets(n, ex.num_vars, hf.L).total_words);
+}
+
+// A transcript's header, parsed and checked for self-consistency (not against a proof).
+struct TranscriptInfo {
+  int L = 0, n = 0, K = 0, d = 0, mode = 0, done = 0;
+  uint64_t expr_digest = 0, field_digest = 0, tag = 0;
+};
+
+inline int transcript_parse(const uint32_t* t, uint64_t words, TranscriptInfo* out) {
+  if (!t) return fail(SC_ERR_INVALID, "NULL transcript");
+  if (words < static_cast<uint64_t>(kTranscriptHeader) || t[kTwMagic] != kTranscriptMagic ||
+      t[kTwHeaderWords] != static_cast<uint32_t>(kTranscriptHeader))
+    return fail(SC_ERR_INVALID, "not a transcript (bad magic or header)");
+  TranscriptInfo I;
+  I.L = static_cast<int>(t[kTwLimbs]);
+  I.n = static_cast<int>(t[kTwRounds]);
+  I.K = static_cast<int>(t[kTwVars]);
+  I.d = static_cast<int>(t[kTwDegree]);
+  I.mode = static_cast<int>(t[kTwMode]);
+  I.done = static_cast<int>(t[kTwDone]);
+  if (!(I.L == 1 || I.L == 2 || I.L == 4 || I.L == 8) || I.n < 1 || I.n > kMaxRounds || I.K < 1 || I.K > kMaxVars ||
+      I.d < 1 || I.d > kMaxPoints - 1 || I.mode < SC_CHALLENGE_SHA3 || I.mode > SC_CHALLENGE_EXPLICIT || I.done < 0 ||
+      I.done > I.n)
+    return fail(SC_ERR_INVALID, "transcript header out of range");
+  if (t[kTwStateWords] != state_offsets(I.n, I.K, I.L).total_words || words < transcript_words(I.n, I.K, I.L))
+    return fail(SC_ERR_INVALID, "transcript of %llu words is shorter than its header says",
+                static_cast<unsigned long long>(words));
+  I.expr_digest = tw_get64(t, kTwExprDigest);
+  I.field_digest = tw_get64(t, kTwFieldDigest);
+  I.tag = tw_get64(t, kTwTablesTag);
+  *out = I;
+  return SC_OK;
+}
+
+// The transcript belongs to this field and expression.
+inline int transcript_match(const TranscriptInfo& I, const HostField& hf, const sc_expr& ex) {
+  if (I.L != hf.L || I.field_digest != field_digest(hf)) return fail(SC_ERR_INVALID, "transcript is of another field");
+  if (I.K != ex.num_vars || I.d != ex.degree || I.expr_digest != expr_digest(ex))
+    return fail(SC_ERR_INVALID, "transcript is of another expression");
+  return SC_OK;
+}
+
+// Proves rounds [first, stop) of a proof on the context's stream. state_io (host,
+// state_offsets words) is uploaded before -- the state after round first - 1, zeros for
+// first = 0 -- and downloaded after. T_0 is first folded up to T_{first-1} with the
+// recorded challenges. Defined in capi.cu.
+int prove_segment(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int n, const uint32_t* tables, int mode,
+                  const uint32_t* explicit_ch, int first, int stop, uint32_t* state_io);
+
+// Folds T_0 (tables) to T_{j-1} on `stream` with r_0..r_{j-2} from chals_dev (L words each):
+// T_i goes to fold_a for odd i and fold_b for even i, where round j's kernel reads it.
+// Nothing to do for j <= 1. Defined in capi.cu.
+int resume_folds(const sc_field* field, int n, int num_tables, const uint32_t* tables, uint32_t* fold_a,
+                 uint32_t* fold_b, const uint32_t* chals_dev, int j, int sm_count, cudaStream_t stream);
+
 }  // namespace sc_host

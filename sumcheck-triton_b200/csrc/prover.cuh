@@ -623,6 +623,36 @@ __global__ void __launch_bounds__(kernel_threads(L), round_min_blocks(L, SHAPE))
   }
 }
 
+// ------------------------------------------------------------------------------ resume folds
+//
+// T_i = T_{i-1} + r_{i-1} (odd - even) and nothing else: the folds that bring a resumed
+// proof's tables to the round it continues from (the round kernel folds the last one
+// itself). One thread per output pair of one table: a 16-byte load per limb plane in, an
+// 8-byte store per plane out, as the round kernel's fused fold. src_len >= 4 entries.
+template <int L, int K>
+__global__ void __launch_bounds__(256) fold_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                                   uint64_t src_len, int num_tables, const uint32_t* r_dev,
+                                                   const FieldParams<L, K> F) {
+  const uint64_t quads = src_len >> 2;  // output pairs per table
+  const uint64_t total = quads * static_cast<uint64_t>(num_tables);
+  const uint64_t dst_len = src_len >> 1;
+  const Fe<L> r = ld_fe_cg<L>(r_dev);
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t k = i / quads, q = i - k * quads;
+    Fe<L> x0, x1, x2, x3;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4*>(src + (k * L + l) * src_len) + q);
+      x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
+    }
+    const Fe<L> e = fe_add(x0, fe_mul(r, fe_sub(x1, x0, F), F), F);
+    const Fe<L> o = fe_add(x2, fe_mul(r, fe_sub(x3, x2, F), F), F);
+#pragma unroll
+    for (int l = 0; l < L; ++l) reinterpret_cast<uint2*>(dst + (k * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+  }
+}
+
 // ------------------------------------------------------------------------------ batched
 //
 // Many independent proofs advance together, one launch per "tick" and degree class: a

@@ -27,6 +27,14 @@
 //
 // The FIFO-plain policy is the baseline: one request at a time, tables generated, then the
 // plain per-round path (sc_prove).
+//
+// Suspension: a request marked by sc_server_suspend leaves at its next round boundary -- the
+// first tick that finds its current round not yet started issues nothing for it and instead
+// queues its state copy and block free, as for a finished request -- and is published with
+// SC_SUSPENDED and its state words (its transcript). A resumed request (submit_resume)
+// starts from such a state: admission uploads it instead of zeroing, regenerates the tables
+// from the seed and refolds them with the recorded challenges to the round it continues from.
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -62,6 +70,14 @@ struct ServeRequest {
   // results (written by the worker before status leaves PENDING)
   std::vector<uint32_t> polys, chals, finals, claim0;
   uint64_t checksum = 0;
+  // transcripts: the round it starts from and that state (resumed requests); the suspend
+  // mark; the state it was suspended with (state words, rounds done)
+  int first = 0;
+  std::vector<uint32_t> resume_state;
+  std::atomic<bool> suspend{false};
+  bool suspending = false;  // worker: leaving with this tick
+  std::vector<uint32_t> suspended_state;
+  int suspended_done = 0;
   // device residence (worker only)
   StateOffsets so{};
   char* block = nullptr;
@@ -160,6 +176,8 @@ struct sc_server {
   std::unordered_map<uint64_t, std::unique_ptr<ServeRequest>> reqs;
   uint64_t next_id = 1;
   uint64_t open_requests = 0;      // submitted and not yet completed or failed
+  uint64_t suspend_epoch = 0;      // sc_server_suspend calls; the worker scans its queue when it moved
+  uint64_t seen_epoch = 0;
   bool stop = false;
   sc_server_stats stats{};
   // worker only
@@ -232,6 +250,8 @@ void publish(sc_server* S, ServeRequest* R, int status, double t_done) {
   R->t_done = t_done;
   if (status == SC_OK)
     ++S->stats.completed;
+  else if (status == SC_SUSPENDED)
+    ++S->stats.suspended;
   else
     ++S->stats.failed;
   --S->open_requests;
@@ -281,10 +301,15 @@ int retire_ticks(sc_server* S, bool block) {
     for (ServeRequest* R : T.completing) {
       const uint32_t* hs = S->stage_host + static_cast<size_t>(R->slot) * S->stage_words;
       const uint32_t dev_status = hs[R->so.status];
-      extract_results(S, R, hs);
+      if (R->suspending && !dev_status) {
+        R->suspended_state.assign(hs, hs + R->so.total_words);
+        R->suspended_done = R->round;
+      } else {
+        extract_results(S, R, hs);
+      }
       S->free_stage.push_back(R->slot);
       R->slot = -1;
-      publish(S, R, dev_status ? SC_ERR_DEVICE : SC_OK, t);
+      publish(S, R, dev_status ? SC_ERR_DEVICE : (R->suspending ? SC_SUSPENDED : SC_OK), t);
     }
     T.completing.clear();
     T.busy = false;
@@ -314,7 +339,10 @@ int retire_ticks(sc_server* S, bool block) {
 // block per tile, so the small requests' higher-priority launches take SMs as these blocks
 // retire), result copy, free, completion event -- all ordered on the lane.
 int issue_large(sc_server* S, ServeRequest* R) {
-  SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->lane));
+  if (R->first)
+    SC_CUDA(cudaMemcpyAsync(R->state, R->resume_state.data(), R->so.total_words * 4, cudaMemcpyHostToDevice, S->lane));
+  else
+    SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->lane));
   ExprDev& E = S->expr_host[R->slot];
   build_expr(S, R->expr, E);
   SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->lane));
@@ -327,7 +355,7 @@ int issue_large(sc_server* S, ServeRequest* R) {
   // blocks still find SMs within microseconds, as hundreds of lane blocks retire in turn).
   constexpr uint64_t kLaneWaves = 4;
   std::vector<uint64_t> tiles(R->n);
-  for (int t = 0; t < R->n; ++t) {
+  for (int t = R->first; t < R->n; ++t) {
     BatchRound& B = rh[t];
     std::memset(&B, 0, sizeof(B));
     round_args(S, *R, t, B.args);
@@ -343,11 +371,14 @@ int issue_large(sc_server* S, ServeRequest* R) {
     B.item_base = 0;
     B.round_items = static_cast<int32_t>(items);
   }
-  SC_CUDA(cudaMemcpyAsync(R->rounds_dev, rh, static_cast<size_t>(R->n) * sizeof(BatchRound), cudaMemcpyHostToDevice,
-                          S->lane));
+  SC_CUDA(cudaMemcpyAsync(R->rounds_dev + R->first, rh + R->first,
+                          static_cast<size_t>(R->n - R->first) * sizeof(BatchRound), cudaMemcpyHostToDevice, S->lane));
   int rc = sc_tables_generate(S->lane_ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
+  if (!rc)
+    rc = resume_folds(S->field, R->n, R->K, R->tables, R->fold_a, R->fold_b, R->state + R->so.chals, R->first,
+                      S->lane_ctx->sm_count, S->lane);
   if (rc) return rc;
-  for (int t = 0; t < R->n; ++t) {
+  for (int t = R->first; t < R->n; ++t) {
     BatchTickArgs A;
     A.rounds = R->rounds_dev + t;
     A.items = nullptr;
@@ -368,6 +399,26 @@ int issue_large(sc_server* S, ServeRequest* R) {
   return SC_OK;
 }
 
+// Queued requests marked for suspension leave where they stand: the state they were
+// submitted with (zeros, or the transcript they resume).
+void suspend_waiting(sc_server* S) {
+  for (auto it = S->waiting.begin(); it != S->waiting.end();) {
+    ServeRequest* R = *it;
+    if (!R->suspend.load()) {
+      ++it;
+      continue;
+    }
+    it = S->waiting.erase(it);
+    if (R->first)
+      R->suspended_state = R->resume_state;
+    else
+      R->suspended_state.assign(R->so.total_words, 0u);
+    R->suspended_done = R->first;
+    R->suspending = true;
+    publish(S, R, SC_SUSPENDED, S->now());
+  }
+}
+
 int admit(sc_server* S) {
   while (!S->waiting.empty() && static_cast<int>(S->active.size() + S->lane_inflight.size()) < S->max_inflight &&
          !S->free_stage.empty()) {
@@ -375,7 +426,7 @@ int admit(sc_server* S) {
     if (S->admitted_bytes + R->footprint > S->budget) break;  // arrival order: no overtaking
     S->waiting.pop_front();
     const BlockLayout b = block_layout(R->n, R->K, S->L, S->tile_pairs);
-    const uint64_t items0 = ((uint64_t{1} << R->n) / 2 + S->tile_pairs - 1) / S->tile_pairs;
+    const uint64_t items0 = (((uint64_t{1} << R->n) >> (R->first + 1)) + S->tile_pairs - 1) / S->tile_pairs;
     R->large = static_cast<int64_t>(items0) > S->large_items;
     cudaStream_t st = R->large ? S->lane : S->stream;
     void* p = nullptr;
@@ -397,7 +448,7 @@ int admit(sc_server* S) {
     R->fold_b = reinterpret_cast<uint32_t*>(R->block + b.fold_b);
     R->slot = S->free_stage.back();
     S->free_stage.pop_back();
-    R->round = 0;
+    R->round = R->first;
     R->issued = 0;
     R->t_admit = S->now();
     S->admitted_bytes += R->footprint;
@@ -406,11 +457,18 @@ int admit(sc_server* S) {
       int rc = issue_large(S, R);
       if (rc) return rc;
     } else {
-      SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->stream));
+      if (R->first)
+        SC_CUDA(cudaMemcpyAsync(R->state, R->resume_state.data(), R->so.total_words * 4, cudaMemcpyHostToDevice,
+                                S->stream));
+      else
+        SC_CUDA(cudaMemsetAsync(R->state, 0, R->so.total_words * 4, S->stream));
       ExprDev& E = S->expr_host[R->slot];
       build_expr(S, R->expr, E);
       SC_CUDA(cudaMemcpyAsync(R->expr_dev, &E, sizeof(ExprDev), cudaMemcpyHostToDevice, S->stream));
       int rc = sc_tables_generate(S->ctx, S->field, R->K, R->n, R->kinds.data(), R->seed, R->tables);
+      if (!rc)
+        rc = resume_folds(S->field, R->n, R->K, R->tables, R->fold_a, R->fold_b, R->state + R->so.chals, R->first,
+                          S->ctx->sm_count, S->stream);
       if (rc) return rc;
       S->active.push_back(R);
     }
@@ -432,6 +490,14 @@ int issue_tick(sc_server* S, bool* issued) {
     if (rc) return rc;
   }
   const double b0 = S->now();
+  // requests marked for suspension whose current round has not started leave with this tick
+  std::vector<ServeRequest*> suspend_now;
+  for (ServeRequest* R : S->active)
+    if (R->issued == 0 && R->suspend.load()) suspend_now.push_back(R);
+  for (ServeRequest* R : suspend_now) {
+    R->suspending = true;
+    S->active.erase(std::find(S->active.begin(), S->active.end(), R));
+  }
   const int nc = static_cast<int>(S->classes.size());
   std::vector<std::vector<BatchRound>> rounds(nc);
   std::vector<std::vector<BatchItem>> items(nc);
@@ -532,7 +598,15 @@ int issue_tick(sc_server* S, bool* issued) {
     SC_CUDA(cudaEventRecord(C.done, C.stream));
     SC_CUDA(cudaStreamWaitEvent(S->stream, C.done, 0));
   }
-  // finished requests: state to pinned staging, block back to the pool
+  // finished and suspended requests: state to pinned staging, block back to the pool
+  for (ServeRequest* R : suspend_now) {
+    SC_CUDA(cudaMemcpyAsync(S->stage_host + static_cast<size_t>(R->slot) * S->stage_words, R->state,
+                            R->so.total_words * 4, cudaMemcpyDeviceToHost, S->stream));
+    SC_CUDA(cudaFreeAsync(R->block, S->stream));
+    R->block = nullptr;
+    S->admitted_bytes -= R->footprint;
+    T.completing.push_back(R);
+  }
   for (ServeRequest* R : done_now) {
     SC_CUDA(cudaMemcpyAsync(S->stage_host + static_cast<size_t>(R->slot) * S->stage_words, R->state,
                             R->so.total_words * 4, cudaMemcpyDeviceToHost, S->stream));
@@ -574,6 +648,7 @@ void fail_all(sc_server* S, int rc) {
 
 void loop_continuous(sc_server* S) {
   bool lane_only = false;  // last pass: nothing to issue, only the lane in flight
+  bool scan_waiting = false;  // a suspension was asked for since the last pass
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
@@ -586,6 +661,8 @@ void loop_continuous(sc_server* S) {
         S->cv_work.wait_for(lk, std::chrono::microseconds(100), [S] { return S->stop || !S->incoming.empty(); });
         S->stats.wait_s += S->now() - w0;
       }
+      scan_waiting = S->suspend_epoch != S->seen_epoch;
+      S->seen_epoch = S->suspend_epoch;
       while (!S->incoming.empty()) {
         S->waiting.push_back(S->incoming.front());
         S->incoming.pop_front();
@@ -594,6 +671,7 @@ void loop_continuous(sc_server* S) {
         return;
     }
     int rc = retire_ticks(S, false);
+    if (scan_waiting) suspend_waiting(S);
     if (!rc) rc = admit(S);
     bool issued = false;
     if (!rc) rc = issue_tick(S, &issued);
@@ -623,6 +701,13 @@ void loop_fifo(sc_server* S) {
       R = S->incoming.front();
       S->incoming.pop_front();
     }
+    if (R->suspend.load()) {  // not started: leaves as submitted
+      R->suspended_state = R->first ? R->resume_state : std::vector<uint32_t>(R->so.total_words, 0u);
+      R->suspended_done = R->first;
+      R->suspending = true;
+      publish(S, R, SC_SUSPENDED, S->now());
+      continue;
+    }
     R->t_admit = S->now();
     mark_busy(S);
     const uint64_t N = uint64_t{1} << R->n;
@@ -640,8 +725,15 @@ void loop_fifo(sc_server* S) {
       R->chals.resize(static_cast<size_t>(R->n) * L);
       R->finals.resize(static_cast<size_t>(1 + R->K) * L);
       R->claim0.resize(L);
-      rc = sc_prove(S->ctx, S->field, &R->expr, R->n, static_cast<const uint32_t*>(p), R->mode, nullptr,
-                    R->polys.data(), R->chals.data(), R->finals.data(), R->claim0.data(), &R->checksum);
+      if (R->first) {  // resumed: the rest of the proof from its transcript's state
+        std::vector<uint32_t> st = R->resume_state;
+        rc = prove_segment(S->ctx, S->field, &R->expr, R->n, static_cast<const uint32_t*>(p), R->mode, nullptr,
+                           R->first, R->n, st.data());
+        if (!rc) extract_results(S, R, st.data());
+      } else {
+        rc = sc_prove(S->ctx, S->field, &R->expr, R->n, static_cast<const uint32_t*>(p), R->mode, nullptr,
+                      R->polys.data(), R->chals.data(), R->finals.data(), R->claim0.data(), &R->checksum);
+      }
     }
     if (p) cudaFreeAsync(p, S->stream);
     {
@@ -844,8 +936,13 @@ int sc_server_footprint(const sc_server* S, const sc_expr* expr, int num_rounds,
   return SC_OK;
 }
 
-int sc_server_submit(sc_server* S, const sc_expr* expr, int num_rounds, const int32_t* table_kinds, uint64_t seed,
-                     int challenge_mode, uint64_t* out_id) {
+}  // extern "C"
+
+namespace {
+
+// Queues a request; `resume` (state words) and `first` continue a transcript.
+int submit_request(sc_server* S, const sc_expr* expr, int num_rounds, const int32_t* table_kinds, uint64_t seed,
+                   int challenge_mode, int first, const uint32_t* resume, uint64_t* out_id) {
   if (!S || !expr || !table_kinds || !out_id) return fail(SC_ERR_INVALID, "NULL argument");
   if (challenge_mode != SC_CHALLENGE_SHA3 && challenge_mode != SC_CHALLENGE_FIXED)
     return fail(SC_ERR_INVALID, "served proofs derive their challenges: SHA3 or fixed mode");
@@ -866,6 +963,8 @@ int sc_server_submit(sc_server* S, const sc_expr* expr, int num_rounds, const in
   R->mode = challenge_mode;
   R->footprint = fp;
   R->so = state_offsets(num_rounds, R->K, S->L);
+  R->first = first;
+  if (first) R->resume_state.assign(resume, resume + R->so.total_words);
   std::lock_guard<std::mutex> lk(S->mu);
   if (S->stop) return fail(SC_ERR_INVALID, "server is shutting down");
   R->id = S->next_id++;
@@ -876,6 +975,65 @@ int sc_server_submit(sc_server* S, const sc_expr* expr, int num_rounds, const in
   ++S->stats.submitted;
   ++S->open_requests;
   S->cv_work.notify_one();
+  return SC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sc_server_submit(sc_server* S, const sc_expr* expr, int num_rounds, const int32_t* table_kinds, uint64_t seed,
+                     int challenge_mode, uint64_t* out_id) {
+  return submit_request(S, expr, num_rounds, table_kinds, seed, challenge_mode, 0, nullptr, out_id);
+}
+
+int sc_server_submit_resume(sc_server* S, const sc_expr* expr, const int32_t* table_kinds, uint64_t seed,
+                            const uint32_t* transcript, uint64_t words, uint64_t* out_id) {
+  if (!S || !expr || !table_kinds || !out_id) return fail(SC_ERR_INVALID, "NULL argument");
+  TranscriptInfo I;
+  int rc = transcript_parse(transcript, words, &I);
+  if (!rc) rc = transcript_match(I, S->field->hf, *expr);
+  if (rc) return rc;
+  if (I.done == I.n) return fail(SC_ERR_INVALID, "the transcript's proof is complete");
+  if (I.tag != seeded_tables_tag(expr->num_vars, table_kinds, seed))
+    return fail(SC_ERR_INVALID, "the transcript is of other tables (table kinds or seed differ)");
+  const uint32_t* state = transcript + kTranscriptHeader;
+  const StateOffsets so = state_offsets(I.n, I.K, I.L);
+  if (state[so.counter] || state[so.status]) return fail(SC_ERR_INVALID, "transcript state records a device error");
+  return submit_request(S, expr, I.n, table_kinds, seed, I.mode, I.done, state, out_id);
+}
+
+int sc_server_suspend(sc_server* S, uint64_t id) {
+  if (!S) return fail(SC_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (id == 0) {
+    for (auto& kv : S->reqs)
+      if (kv.second->status == SC_ERR_PENDING) kv.second->suspend.store(true);
+  } else {
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return fail(SC_ERR_INVALID, "unknown request %llu", static_cast<unsigned long long>(id));
+    it->second->suspend.store(true);
+  }
+  ++S->suspend_epoch;
+  S->cv_work.notify_all();
+  return SC_OK;
+}
+
+int sc_server_transcript(sc_server* S, uint64_t id, uint32_t* transcript, uint64_t words) {
+  if (!S || !transcript) return fail(SC_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return fail(SC_ERR_INVALID, "unknown request %llu", static_cast<unsigned long long>(id));
+  const ServeRequest* R = it->second.get();
+  if (R->status != SC_SUSPENDED)
+    return fail(R->status == SC_ERR_PENDING ? SC_ERR_PENDING : SC_ERR_INVALID,
+                "request %llu is not suspended (status %d)", static_cast<unsigned long long>(id), R->status);
+  const size_t need = transcript_words(R->n, R->K, S->L);
+  if (words < need)
+    return fail(SC_ERR_INVALID, "transcript needs %zu words, got %llu", need, static_cast<unsigned long long>(words));
+  transcript_header(transcript, S->field->hf, R->expr, R->n, R->mode, R->suspended_done,
+                    seeded_tables_tag(R->K, R->kinds.data(), R->seed));
+  std::memcpy(transcript + kTranscriptHeader, R->suspended_state.data(), R->suspended_state.size() * 4);
   return SC_OK;
 }
 
@@ -890,6 +1048,7 @@ int sc_server_wait(sc_server* S, uint64_t id, int timeout_ms) {
     S->cv_done.wait(lk, ready);
   else if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
     return fail(SC_ERR_TIMEOUT, "request %llu not done after %d ms", static_cast<unsigned long long>(id), timeout_ms);
+  if (R->status == SC_SUSPENDED) return SC_SUSPENDED;
   if (R->status != SC_OK) return fail(R->status, "request %llu failed with status %d", static_cast<unsigned long long>(id), R->status);
   return SC_OK;
 }
@@ -913,6 +1072,8 @@ int sc_server_result(sc_server* S, uint64_t id, uint32_t* out_round_polys, uint3
   if (it == S->reqs.end()) return fail(SC_ERR_INVALID, "unknown request %llu", static_cast<unsigned long long>(id));
   const ServeRequest* R = it->second.get();
   if (R->status == SC_ERR_PENDING) return fail(SC_ERR_PENDING, "request %llu has not completed", static_cast<unsigned long long>(id));
+  if (R->status == SC_SUSPENDED)
+    return fail(SC_SUSPENDED, "request %llu was suspended: read its transcript", static_cast<unsigned long long>(id));
   if (R->status != SC_OK) return fail(R->status, "request %llu failed with status %d", static_cast<unsigned long long>(id), R->status);
   if (out_round_polys) std::memcpy(out_round_polys, R->polys.data(), R->polys.size() * 4);
   if (out_challenges) std::memcpy(out_challenges, R->chals.data(), R->chals.size() * 4);

@@ -20,6 +20,7 @@ from .api import (
 )
 from .expression import encode_expression, expression_degree, expression_vars, normalize_expression
 from .fields import FIELD_SPECS, FieldSpec, UnsafeModulusError, check_montgomery_modulus, get_field
+from .transcript import Transcript
 from .workloads import KERNEL_WORKLOADS, WORKLOADS, get_kernel_workload, get_workload
 
 __all__ = [
@@ -29,6 +30,7 @@ __all__ = [
     "FieldSpec",
     "KERNEL_WORKLOADS",
     "Proof",
+    "Transcript",
     "UnsafeModulusError",
     "WORKLOADS",
     "available_backends",

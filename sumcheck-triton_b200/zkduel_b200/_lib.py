@@ -24,6 +24,7 @@ SC_ERR_DEVICE = 5
 SC_ERR_NOMEM = 6
 SC_ERR_TIMEOUT = 7
 SC_ERR_PENDING = 8
+SC_SUSPENDED = 9
 
 SC_SERVE_CONTINUOUS = 0
 SC_SERVE_FIFO_PLAIN = 1
@@ -47,7 +48,8 @@ class ServerStats(ctypes.Structure):
     """sc_server_stats."""
 
     _fields_ = [
-        ("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("ticks", c_uint64),
+        ("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("suspended", c_uint64),
+        ("ticks", c_uint64),
         ("items", c_uint64), ("peak_inflight", c_uint64), ("peak_footprint", c_uint64), ("budget", c_uint64),
         ("busy_s", c_double), ("alloc_s", c_double), ("wait_s", c_double), ("build_s", c_double),
     ]
@@ -119,6 +121,15 @@ SIGNATURES = {
     "sc_server_times": (c_int, [c_void_p, c_uint64, F64P, F64P, F64P]),
     "sc_server_release": (c_int, [c_void_p, c_uint64]),
     "sc_server_stats_get": (c_int, [c_void_p, POINTER(ServerStats)]),
+    "sc_server_suspend": (c_int, [c_void_p, c_uint64]),
+    "sc_server_transcript": (c_int, [c_void_p, c_uint64, U32P, c_uint64]),
+    "sc_server_submit_resume": (c_int, [c_void_p, c_void_p, POINTER(c_int32), c_uint64, U32P, c_uint64, U64P]),
+    "sc_transcript_words": (c_int, [c_void_p, c_void_p, c_int, U64P]),
+    "sc_transcript_init": (c_int, [c_void_p, c_void_p, c_int, c_int, c_uint64, U32P, c_uint64]),
+    "sc_transcript_info": (c_int, [U32P, c_uint64, POINTER(c_int), POINTER(c_int), POINTER(c_int), U64P]),
+    "sc_transcript_result": (c_int, [c_void_p, c_void_p, U32P, c_uint64, U32P, U32P, U32P, U32P, U64P]),
+    "sc_tables_tag": (c_int, [c_int, POINTER(c_int32), c_uint64, U64P]),
+    "sc_prove_resume": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, U32P, c_int, U32P, c_uint64]),
     "sc_server_destroy": (c_int, [c_void_p]),
     "sc_prove": (
         c_int,

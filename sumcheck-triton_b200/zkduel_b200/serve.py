@@ -13,6 +13,11 @@ baseline: one request at a time, in arrival order, through the plain per-round p
 A request's result is bit-identical to ``prove_device`` on ``generate_tables`` with the
 same seed, alone or in any mix; the GPU tests check exactly that.
 
+``suspend`` stops requests at their next round boundary and frees their device memory;
+``transcript`` then gives each one's :class:`~zkduel_b200.transcript.Transcript`, which
+``submit(..., resume=t)`` continues -- on this server, another one, or after a restart --
+or ``transcript.prove_rounds`` finishes on the plain path, bit-identically either way.
+
 ``replay`` drives a server with an arrival trace (seconds from its start) and returns the
 latency of every request: completion minus arrival, on the server's clock.
 """
@@ -30,6 +35,7 @@ from . import _lib
 from .api import CompiledExpression, Proof, get_device_field
 from .expression import encode_expression
 from .fields import FieldSpec, get_field
+from .transcript import Transcript
 
 
 @dataclass
@@ -64,7 +70,7 @@ class ProofServer:
                                   int(chunk_items), ctypes.byref(h))
         _lib.check(rc, "sc_server_create")
         self.handle = h
-        self._meta: dict[int, tuple] = {}  # id -> (n, degree, num_tables, var names)
+        self._meta: dict[int, tuple] = {}  # id -> (n, degree, num_tables, var names, compiled expression)
         self._exprs: dict = {}
 
     # -------------------------------------------------------------------- requests
@@ -92,23 +98,56 @@ class ProofServer:
         return out.value
 
     def submit(self, expression, num_vars: int, seed: int, kinds: Sequence[int] | None = None,
-               challenge_mode: str = "sha3") -> int:
-        """Queues one request; returns its id at once."""
+               challenge_mode: str = "sha3", resume: Transcript | None = None) -> int:
+        """Queues one request; returns its id at once. ``resume``: continue that transcript
+        (same expression, num_vars, seed and kinds as its tables; its challenge mode)."""
         ce = self._compiled(expression)
         k = ce.num_vars
         kinds = [_lib.SC_TABLE_UNIFORM] * k if kinds is None else list(kinds)
         if len(kinds) != k:
             raise ValueError(f"{len(kinds)} table kinds for {k} tables")
-        mode = _lib.CHALLENGE_MODES[challenge_mode]
         rid = ctypes.c_uint64(0)
-        rc = _lib.load().sc_server_submit(self.handle, ce.handle, int(num_vars), _lib.i32_array(kinds),
-                                          ctypes.c_uint64(int(seed) & (2**64 - 1)), mode, ctypes.byref(rid))
-        _lib.check(rc, "sc_server_submit")
-        self._meta[rid.value] = (int(num_vars), ce.degree, k, tuple(ce.encoded.var_names))
+        seed_c = ctypes.c_uint64(int(seed) & (2**64 - 1))
+        if resume is not None:
+            if resume.num_rounds != int(num_vars):
+                raise ValueError(f"transcript has {resume.num_rounds} rounds, request {num_vars}")
+            w = resume.words
+            rc = _lib.load().sc_server_submit_resume(self.handle, ce.handle, _lib.i32_array(kinds), seed_c,
+                                                     w.ctypes.data_as(_lib.U32P), w.size, ctypes.byref(rid))
+            _lib.check(rc, "sc_server_submit_resume")
+        else:
+            mode = _lib.CHALLENGE_MODES[challenge_mode]
+            rc = _lib.load().sc_server_submit(self.handle, ce.handle, int(num_vars), _lib.i32_array(kinds), seed_c,
+                                              mode, ctypes.byref(rid))
+            _lib.check(rc, "sc_server_submit")
+        self._meta[rid.value] = (int(num_vars), ce.degree, k, tuple(ce.encoded.var_names), ce)
         return rid.value
 
-    def wait(self, rid: int, timeout_ms: int = -1) -> None:
-        _lib.check(_lib.load().sc_server_wait(self.handle, ctypes.c_uint64(rid), int(timeout_ms)), "sc_server_wait")
+    def wait(self, rid: int, timeout_ms: int = -1) -> str:
+        """Waits for request ``rid``: "done" or "suspended" (raises if it failed or timed out)."""
+        rc = _lib.load().sc_server_wait(self.handle, ctypes.c_uint64(rid), int(timeout_ms))
+        if rc == _lib.SC_SUSPENDED:
+            return "suspended"
+        _lib.check(rc, "sc_server_wait")
+        return "done"
+
+    def suspend(self, rid: int | None = None) -> None:
+        """Suspends request ``rid`` (None: every unfinished request) at its next round boundary."""
+        _lib.check(_lib.load().sc_server_suspend(self.handle, ctypes.c_uint64(0 if rid is None else rid)),
+                   "sc_server_suspend")
+
+    def transcript(self, rid: int) -> Transcript:
+        """The transcript of a suspended request."""
+        if rid not in self._meta:
+            raise ValueError(f"unknown request {rid}")
+        n, _d, _k, _names, ce = self._meta[rid]
+        lib = _lib.load()
+        words = ctypes.c_uint64(0)
+        _lib.check(lib.sc_transcript_words(self.field.handle, ce.handle, n, ctypes.byref(words)), "sc_transcript_words")
+        w = np.zeros(words.value, dtype=np.uint32)
+        _lib.check(lib.sc_server_transcript(self.handle, ctypes.c_uint64(rid), w.ctypes.data_as(_lib.U32P), w.size),
+                   "sc_server_transcript")
+        return Transcript(w)
 
     def drain(self, timeout_ms: int = -1) -> None:
         _lib.check(_lib.load().sc_server_drain(self.handle, int(timeout_ms)), "sc_server_drain")
@@ -116,7 +155,7 @@ class ProofServer:
     def result(self, rid: int) -> Proof:
         if rid not in self._meta:
             raise ValueError(f"unknown request {rid}")
-        n, d, k, names = self._meta[rid]
+        n, d, k, names, _ce = self._meta[rid]
         L = self.spec.limbs
         polys = np.zeros((n, d + 1, L), dtype=np.uint32)
         chals = np.zeros((n, L), dtype=np.uint32)
