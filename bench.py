@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--path", choices=["batched", "plain"], default="batched")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-chunks", type=int, default=16,
+                    help="host-buffer path: batches whose copies overlap the proving of the ones before")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuned ones")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference CUDA executable comparison")
@@ -507,7 +509,7 @@ def main() -> int:
         line["roofline"] = roof
 
     if rank == 0 and world == 1 and not args.no_e2e:
-        line["e2e"] = e2e_measure(work, args, device, batcher if path == "batched" else None)
+        line["e2e"] = e2e_measure(work, args, device, path == "batched", tuning)
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0, sample_stride=4)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
@@ -621,50 +623,27 @@ def served_measure(args, device, rank: int, world: int) -> dict:
     return out
 
 
-def e2e_measure(work: Workload, args, device, batcher=None) -> dict:
+def e2e_measure(work: Workload, args, device, batched: bool, tuning=None) -> dict:
     """Host-buffer path: per step, every proof's canonical tables go from pinned host memory
     to the device and are converted to Montgomery form there; the proofs run (batched, or
     one sc_prove per proof); every proof's results are read back to the host."""
-    import ctypes
-
     import torch
 
-    from zkduel_b200 import _lib, api
+    from zkduel_b200 import api
+    from zkduel_b200.batch import HostBatchProver
 
     host = []
     for s, spec, _e, t in work.items:
         canon = api.download_tables(t, spec)
         host.append(torch.from_numpy(canon.view("int32")).pin_memory())
     h2d = sum(h.numel() * 4 for h in host)
-    ctx = api.get_context(device)
-    lib = _lib.load()
 
-    if batcher is not None:
-        # the copies spread over E2E_COPY_STREAMS streams (each with its own context for the
-        # conversion), joined into the proving stream before the batch runs
-        nstreams = int(os.environ.get("E2E_COPY_STREAMS", "3"))
-        streams = [torch.cuda.Stream(device) for _ in range(nstreams)]
-        ctxs = []
-        for st in streams:
-            with torch.cuda.stream(st):
-                ctxs.append(api.get_context(device))
-
-        def step():
-            main = torch.cuda.current_stream(device)
-            for st in streams:
-                st.wait_stream(main)
-            for i, ((s, spec, _e, t), h) in enumerate(zip(work.items, host)):
-                st, c = streams[i % nstreams], ctxs[i % nstreams]
-                with torch.cuda.stream(st):
-                    t.copy_(h, non_blocking=True)
-                fld = api.get_device_field(spec, ctx.device)
-                K, _L, N = t.shape
-                _lib.check(lib.sc_tables_to_mont(c.handle, fld.handle, ctypes.c_void_p(t.data_ptr()),
-                                                 ctypes.c_uint64(N), int(K)), "sc_tables_to_mont")
-            for st in streams:
-                main.wait_stream(st)
-            batcher.run()
-            return batcher.results()
+    if batched:
+        # the public host-buffer batch API: copies in chunks overlapped with the proving
+        hb = HostBatchProver([(e, spec.bit_width, s.num_vars) for s, spec, e, _t in work.items], host,
+                             chunks=args.e2e_chunks, copy_streams=int(os.environ.get("E2E_COPY_STREAMS", "1")),
+                             device=device, tuning=tuning)
+        step = hb.run
     else:
         def step():
             return [api.prove_host(h, e, spec, s.num_vars, "sha3", device=device)
@@ -680,9 +659,31 @@ def e2e_measure(work: Workload, args, device, batcher=None) -> dict:
     dt = (time.perf_counter() - t0) / steps
     d2h = sum(p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
               for p in res)
+    pcie = h2d_bandwidth(device)
     return {"value": STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": dt * 1e3, "path": ("batched" if batcher is not None else "plain") + " (host buffers)",
-            "steps": steps, "timer": "host wall clock around synchronised steps"}
+            "ms_per_step": dt * 1e3,
+            "path": (f"batched, {args.e2e_chunks} chunks" if batched else "plain") + " (host buffers)",
+            "steps": steps, "timer": "host wall clock around synchronised steps",
+            # the bound of this path: the step's host-to-device bytes at the measured copy rate
+            "pcie_h2d_gbs": pcie, "h2d_frac": (h2d / dt / 1e9) / pcie if pcie else None}
+
+
+def h2d_bandwidth(device, nbytes: int = 1 << 30) -> float:
+    """Pinned host-to-device copy rate (GB/s): best of 3 copies of 1 GiB, host timer around
+    synchronised copies."""
+    import torch
+
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    best = 0.0
+    for _ in range(3):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        d.copy_(h, non_blocking=True)
+        torch.cuda.synchronize(device)
+        best = max(best, nbytes / (time.perf_counter() - t0) / 1e9)
+    del h, d
+    return best
 
 
 if __name__ == "__main__":

@@ -135,3 +135,20 @@ def test_tune_for_keeps_results_and_reports_timings():
     bp.run()
     for i, s in enumerate(specs):
         _same(bp.result(i), api.prove_device(items[i][3], s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 7])
+def test_host_batch_prover_equals_single_proofs(chunks):
+    from zkduel_b200.batch import HostBatchProver
+
+    specs = _mixed(30, 2, 14, 21)
+    dev = [_tables(get_field(s.bit_width), s) for s in specs]
+    host = [torch.from_numpy(api.download_tables(t, get_field(s.bit_width)).view(np.int32)).pin_memory()
+            for s, t in zip(specs, dev)]
+    hb = HostBatchProver([(s.expression, s.bit_width, s.num_vars) for s in specs], host, chunks=chunks)
+    assert len(hb.chunks) == min(chunks, len(specs))
+    for _ in range(2):  # the second run reuses the device tables
+        res = hb.run()
+        for s, t, p in zip(specs, dev, res):
+            _same(p, api.prove_device(t, s.expression, get_field(s.bit_width), s.num_vars, "sha3"))
+    hb.close()
