@@ -428,13 +428,15 @@ def main() -> int:
     if path == "batched":
         # Degree classes of one field run concurrently on their own streams: a field's
         # kernel time is the union of its ticks' [start, end] intervals (busy time).
+        # a class's work is every round of its proofs (the last tick of a proof also proves its
+        # tail rounds, so ticks and rounds do not map one to one)
         classes = batcher.tick_times()
         spans = {}
         for c in classes:
-            for t, (a, b_) in enumerate(zip(c["start"], c["end"])):
-                b = sum(work_per_round[i][t][1] for i in c["proofs"] if t < len(work_per_round[i]))
-                im = sum(work_per_round[i][t][2] for i in c["proofs"] if t < len(work_per_round[i]))
-                add(c["limbs"], 0.0, b, im)
+            b = sum(w[1] for i in c["proofs"] for w in work_per_round[i])
+            im = sum(w[2] for i in c["proofs"] for w in work_per_round[i])
+            add(c["limbs"], 0.0, b, im, launches=len(c["start"]))
+            for a, b_ in zip(c["start"], c["end"]):
                 spans.setdefault(c["limbs"], []).append((a, b_))
         for L, iv in spans.items():
             iv.sort()

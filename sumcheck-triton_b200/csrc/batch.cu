@@ -20,6 +20,23 @@ using namespace sc_host;
 namespace {
 // Rounds with at least this many pairs derive g(1) from the claim (see capi.cu).
 constexpr uint64_t kBatchSkip1MinPairs = uint64_t{1} << 12;
+// Tail rounds (batch_round_kernel: from a proof's first one-tile round on, that item's block
+// proves the rest of the proof) are off in batches. Measured on B200 with the 512-proof mixed
+// stream: 9.0k proofs/s with tails, 9.9k without. A 256-bit tail of ~10 rounds takes a block
+// ~200 us, longer than the late ticks it replaces (~30-45 us each), and every late tick then
+// holds some proof's tail; without tails the proofs' small rounds overlap within each tick.
+#ifndef SC_BATCH_TAILS
+#define SC_BATCH_TAILS 0
+#endif
+constexpr bool kBatchTails = SC_BATCH_TAILS != 0;
+
+// Ticks proof p takes: one per round, or up to its first one-tile round with tails.
+inline int proof_ticks(int n, uint64_t tile) {
+  if (!kBatchTails) return n;
+  for (int t = 0; t < n; ++t)
+    if ((uint64_t{1} << n) >> (t + 1) <= tile) return t + 1;
+  return n;
+}
 
 struct BatchClass {
   int dclass = 2;
@@ -146,6 +163,9 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
     if ((rc = batch_kernel_setup(L, B->kind, dc, kmax, B->class_threads[ci], ctx->sm_count, &C.threads, &C.grid,
                                  &C.smem)))
       return rc;
+    C.max_rounds = 0;  // ticks of the class
+    for (int p : C.proofs)
+      C.max_rounds = std::max(C.max_rounds, proof_ticks(B->n[p], static_cast<uint64_t>(C.threads) * B->ppt[p]));
     B->classes.push_back(std::move(C));
   }
   // per-proof state and fold buffers (16-byte aligned carve-outs of two pools)
@@ -181,7 +201,9 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
       C.tick_item0.push_back(static_cast<int>(items.size()));
       int tick_items = 0;
       for (int p : C.proofs) {
-        if (t >= B->n[p]) continue;
+        const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt[p];
+        const int ticks = proof_ticks(B->n[p], tile);
+        if (t >= ticks) continue;
         const int n = B->n[p];
         const uint64_t N = uint64_t{1} << n;
         BatchRound R;
@@ -215,7 +237,12 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
         A.st.claim0 = s + o.claim0;
         A.st.claim = s + o.claim;
         R.expr = exprs_dev + p;
-        const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt[p];
+        if (t == ticks - 1 && ticks < n) {
+          R.tail_rounds = n - ticks;
+          R.skip1_min_pairs = static_cast<uint32_t>(kBatchSkip1MinPairs);
+          R.fold_a = pool + fold_a[p];
+          R.fold_b = pool + fold_b[p];
+        }
         const uint64_t nitems = (A.pairs + tile - 1) / tile;
         R.first_item = static_cast<int>(items.size()) - C.tick_item0[t];  // tick-relative
         R.num_items = static_cast<int>(nitems);

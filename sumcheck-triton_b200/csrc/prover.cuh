@@ -663,6 +663,11 @@ __global__ void __launch_bounds__(256) fold_kernel(const uint32_t* __restrict__ 
 // while the other blocks go on with other proofs' items. A round's items may be spread over
 // several ticks (the served prover slices large rounds): the ticket counts to the round's
 // item total, whichever tick its last item runs in.
+//
+// Tail rounds: once a proof's round fits in one item, the block that proves it also proves
+// every later round of that proof (tail_rounds of them), one after another with block
+// barriers in between -- a few microseconds a round instead of one tick each. Round j + 1
+// reads T_j, which this block wrote itself, and r_j, which its warp 0 just derived.
 
 struct BatchRound {
   RoundArgs args;        // this proof's round (src/dst/len/pairs/round/fold/mode/flags/fc/state)
@@ -672,6 +677,10 @@ struct BatchRound {
   int32_t num_items;
   int32_t item_base;     // round-relative index of this tick's first item of the round
   int32_t round_items;   // items of the whole round, over all ticks
+  int32_t tail_rounds;   // > 0: the block that finalises this round proves the next tail_rounds too
+  uint32_t skip1_min_pairs;  // tail rounds: g(1) from the claim when a round has this many pairs
+  uint32_t* fold_a;      // tail rounds: T_i for odd i
+  uint32_t* fold_b;      //              T_i for even i >= 2
 };
 
 struct BatchItem {
@@ -729,31 +738,52 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
       if (tid == 0) cur_expr = R.expr;
     }
     const int d = E.degree;
-    Fe<L> acc[DMAX + 1];
-#pragma unroll
-    for (int t = 0; t <= DMAX; ++t) acc[t] = fe_zero<L>();
-    Fe<L> r_prev = fe_zero<L>();
-    if (R.args.fold) r_prev = ld_fe_cg<L>(R.args.st.chals + (R.args.round - 1) * L);
     uint32_t* sv = smem;
     uint32_t* sd = smem + E.num_vars * L * nthr;
-    process_pairs<L, K, DMAX>(R.args.src, R.args.dst, R.args.src_len, R.args.fold != 0, r_prev, E, sv, sd,
-                              I.start + tid, I.start + I.count, nthr, R.args.skip1 != 0, acc, F);
-    __syncthreads();
-    block_reduce<L, K, DMAX + 1>(acc, d, smem, g_sm, F);
-    uint32_t* slot = R.partials + static_cast<uint64_t>(R.item_base + (it - R.first_item)) * kMaxPoints * L;
-    for (int i = tid; i < (d + 1) * L; i += nthr) slot[i] = g_sm[i];
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.round_items - 1));
-    __syncthreads();
-    if (is_last) {
-      __threadfence();
-      reduce_partials<L, K, DMAX + 1>(R.partials, 0, R.round_items, d, smem, g_sm, F);
+    // k = 0: this item of the proof's round; k >= 1: the proof's tail rounds (only in the
+    // block that finalised round k - 1; R.args then describes round R.args.round)
+    for (int k = 0;; ++k) {
+      Fe<L> acc[DMAX + 1];
+#pragma unroll
+      for (int t = 0; t <= DMAX; ++t) acc[t] = fe_zero<L>();
+      Fe<L> r_prev = fe_zero<L>();
+      if (R.args.fold) r_prev = ld_fe_cg<L>(R.args.st.chals + (R.args.round - 1) * L);
+      const uint64_t q0 = k == 0 ? I.start : 0, q1 = k == 0 ? I.start + I.count : R.args.pairs;
+      process_pairs<L, K, DMAX>(R.args.src, R.args.dst, R.args.src_len, R.args.fold != 0, r_prev, E, sv, sd, q0 + tid,
+                                q1, nthr, R.args.skip1 != 0, acc, F);
+      __syncthreads();
+      block_reduce<L, K, DMAX + 1>(acc, d, smem, g_sm, F);
+      if (k == 0) {
+        uint32_t* slot = R.partials + static_cast<uint64_t>(R.item_base + (it - R.first_item)) * kMaxPoints * L;
+        for (int i = tid; i < (d + 1) * L; i += nthr) slot[i] = g_sm[i];
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) is_last = (atomicAdd(R.args.st.counter, 1u) == static_cast<uint32_t>(R.round_items - 1));
+        __syncthreads();
+        if (!is_last) break;
+        __threadfence();
+        reduce_partials<L, K, DMAX + 1>(R.partials, 0, R.round_items, d, smem, g_sm, F);
+      }
       if (tid < 32) finalize_round<L, K>(R.args, E, F, g_sm, msg);
-      if (tid == 0) {
+      if (k == 0 && tid == 0) {
         __threadfence();
         *R.args.st.counter = 0;
       }
+      if (k == R.tail_rounds) break;
+      __syncthreads();  // the finalisation read R.args; r_j and T_j are visible to the block
+      if (tid == 0) {   // round j + 1 of the same proof
+        RoundArgs& A = R.args;
+        const int j = A.round + 1;
+        if (j >= 2) A.src = A.dst;  // T_j (round 1 folds the tables themselves)
+        A.dst = (j & 1) ? R.fold_a : R.fold_b;
+        A.round = j;
+        A.pairs >>= 1;
+        A.src_len = A.pairs * 4;
+        A.fold = 1;
+        A.skip1 = A.pairs >= R.skip1_min_pairs ? 1 : 0;
+        A.want_claim = (j + 1 < A.num_rounds && (A.pairs >> 1) >= R.skip1_min_pairs) ? 1 : 0;
+      }
+      __syncthreads();
     }
   }
 }
