@@ -11,8 +11,10 @@ seed r, so per-GPU work is fixed: weak scaling, no collective on the data path).
 Prints one JSON line (rank 0):
   value      proofs/s over all ranks, tables resident in HBM before the timed region,
              timed with CUDA events on the proving stream, max over ranks;
-  e2e        the same through the host-buffer API: every step copies each proof's tables
-             from pinned host memory and reads each proof's results back;
+  e2e        the same through the host-buffer API (zkduel_b200.batch.HostBatchProver): every
+             step copies each proof's tables from pinned host memory, in chunks whose copies
+             overlap the proving of the chunks before, and reads each proof's results back;
+             reported with the measured PCIe host-to-device rate that bounds it;
   plain      the same stream proved one proof at a time (the denominator of the batched
              speed-up);
   roofline   the dominant round kernel (by time) against its bound: integer multiply-adds

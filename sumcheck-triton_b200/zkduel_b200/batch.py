@@ -177,6 +177,20 @@ class BatchProver:
             pass
 
 
+def chunk_bounds(sizes: Sequence[int], chunks: int) -> list[int]:
+    """Cuts proofs of ``sizes`` bytes into at most ``chunks`` consecutive runs of about equal
+    bytes: the boundaries [0, ..., len(sizes)], every run non-empty."""
+    n = len(sizes)
+    total, nch = sum(sizes), max(1, min(int(chunks), n))
+    bounds, acc = [0], 0
+    for i, b in enumerate(sizes):
+        acc += b
+        if len(bounds) < nch and acc >= total * len(bounds) / nch and i + 1 < n:
+            bounds.append(i + 1)
+    bounds.append(n)
+    return bounds
+
+
 class HostBatchProver:
     """Proves proofs whose tables live in host memory, end to end.
 
@@ -221,15 +235,9 @@ class HostBatchProver:
             if tuple(h.shape) != tuple(t.shape):
                 raise ValueError(f"host tables {tuple(h.shape)}, expected {tuple(t.shape)}")
             self.dev_tables.append(t)
-        # consecutive chunks of about equal bytes
         sizes = [h.numel() * 4 for h in self.host]
-        total, nch = sum(sizes), max(1, min(int(chunks), len(items)))
-        bounds, acc = [0], 0
-        for i, b in enumerate(sizes):
-            acc += b
-            if len(bounds) < nch and acc >= total * len(bounds) / nch and i + 1 < len(items):
-                bounds.append(i + 1)
-        bounds.append(len(items))
+        total = sum(sizes)
+        bounds = chunk_bounds(sizes, chunks)
         self.chunks = []
         for a, b in zip(bounds[:-1], bounds[1:]):
             sub = [(items[i][0], items[i][1], items[i][2], self.dev_tables[i]) for i in range(a, b)]
