@@ -454,7 +454,15 @@ def main() -> int:
             per_class[L]["ms"] = busy
         gpu_launches = sum(len(c["ms"]) for c in classes) * args.steps
     else:
-        flat = [w for rounds in work_per_round for w in rounds]
+        # one launch per round up to a proof's tail round, then one launch for the rest
+        from zkduel_b200 import api
+
+        flat = []
+        for (s, spec, e, _t), rounds in zip(work.items, work_per_round):
+            _n, tail = api.prove_launches(e, spec, s.num_vars, device)
+            flat.extend(rounds[:tail])
+            if tail < len(rounds):
+                flat.append((spec.limbs, sum(w[1] for w in rounds[tail:]), sum(w[2] for w in rounds[tail:])))
         for i, t in enumerate(launch_ms):
             L, b, im = flat[i % len(flat)]
             add(L, t, b, im)

@@ -151,6 +151,14 @@ int sc_prove(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_ro
              uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
              uint32_t* out_claim0, uint64_t* out_checksum);
 
+/* How sc_prove runs this proof: *out_launches kernel launches (the per-launch timings of
+ * sc_ctx_launch_times come in this number per proof). Rounds before *out_tail_round take a
+ * launch each; from it on (when < num_rounds), the rounds are small enough for one block,
+ * and one launch proves them all, round after round inside that block. No counterpart in
+ * the reference (its executable launches per round and per point). */
+int sc_prove_launches(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,
+                      int* out_launches, int* out_tail_round);
+
 /* sc_prove without any allocation, for callers that cannot call cudaMalloc (code inside
  * another framework's memory pool or under a fixed device-memory budget, plug-ins that may
  * not grow the process's footprint after start-up). No counterpart in the reference.

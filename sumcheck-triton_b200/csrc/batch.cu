@@ -32,9 +32,10 @@ constexpr bool kBatchTails = SC_BATCH_TAILS != 0;
 
 // Ticks proof p takes: one per round, or up to its first one-tile round with tails.
 inline int proof_ticks(int n, uint64_t tile) {
-  if (!kBatchTails) return n;
-  for (int t = 0; t < n; ++t)
-    if ((uint64_t{1} << n) >> (t + 1) <= tile) return t + 1;
+  if constexpr (kBatchTails) {
+    for (int t = 0; t < n; ++t)
+      if ((uint64_t{1} << n) >> (t + 1) <= tile) return t + 1;
+  }
   return n;
 }
 

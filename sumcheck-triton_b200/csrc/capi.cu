@@ -20,6 +20,52 @@ constexpr uint64_t kSkip1MinPairs = uint64_t{1} << 12;
 
 inline bool round_skip1(int n, int j) { return j >= 1 && (uint64_t{1} << (n - j - 1)) >= kSkip1MinPairs; }
 
+// Tail launch: from the first round with at most one pair per thread of the batched kernel's
+// block, that one block proves the rest of the proof (batch_round_kernel's tail rounds: no
+// grid-wide partials and no launch per round). Generic expressions only: the batched kernel
+// has no compile-time shapes, and the shape kernels' small rounds beat its generic evaluator.
+// Measured on B200 (median of 10 proofs): a b over 2^32 - 5, n = 16, 0.254 -> 0.228 ms,
+// n = 8 0.147 -> 0.110 ms; a degree-3 expression over 2^127 - 1, n = 8..20, 1.09-1.36x;
+// with the zerocheck and g(abc + de) shapes, 0.91-1.0x (so those keep a launch per round).
+#ifndef SC_PLAIN_TAILS
+#define SC_PLAIN_TAILS 1
+#endif
+constexpr bool kPlainTails = SC_PLAIN_TAILS != 0;
+
+struct TailDesc {
+  BatchRound r;
+  ExprDev e;
+};
+
+int tail_shape(sc_ctx* ctx, int L, int kind, int dclass, int tables, int* threads, size_t* smem) {
+  for (const TailShape& t : ctx->tail_shapes)
+    if (t.L == L && t.kind == kind && t.dclass == dclass && t.tables == tables) {
+      *threads = t.threads;
+      *smem = t.smem;
+      return SC_OK;
+    }
+  int grid = 0;
+  int rc = batch_kernel_setup(L, kind, dclass, tables, 0, ctx->sm_count, threads, &grid, smem);
+  if (rc) return rc;
+  ctx->tail_shapes.push_back(TailShape{L, kind, dclass, tables, *threads, *smem});
+  return SC_OK;
+}
+
+// The round the tail launch starts at (stop: none), for a proof run up to round stop.
+int tail_round(sc_ctx* ctx, int L, int kind, int dclass, int tables, int shape, int n, int first, int stop,
+               int* out_round, int* threads, size_t* smem) {
+  *out_round = stop;
+  if (!kPlainTails || stop != n || shape != kShapeGeneric) return SC_OK;
+  int rc = tail_shape(ctx, L, kind, dclass, tables, threads, smem);
+  if (rc) return rc;
+  for (int j = first; j < n - 1; ++j)
+    if (((uint64_t{1} << n) >> (j + 1)) <= static_cast<uint64_t>(*threads)) {
+      *out_round = j;
+      break;
+    }
+  return SC_OK;
+}
+
 template <int L, int K, int DMAX>
 struct ProveRun {
   // Rounds [first, stop) of the proof. state_io (host, state words; NULL for a whole proof
@@ -102,6 +148,9 @@ struct ProveRun {
                            st + so.chals, first, ctx->sm_count, ctx->stream)))
       return rc;
     const uint32_t* prev = first <= 1 ? tables : static_cast<const uint32_t*>(((first - 1) & 1) ? ctx->fold_a.p : ctx->fold_b.p);
+    int tail_j = stop, tail_threads = 0;
+    size_t tail_smem = 0;
+    if ((rc = tail_round(ctx, L, K, DMAX, K_, shape, n, first, stop, &tail_j, &tail_threads, &tail_smem))) return rc;
     for (int j = first; j < stop; ++j) {
       A.round = j;
       A.pairs = N >> (j + 1);
@@ -118,6 +167,37 @@ struct ProveRun {
         A.src_len = N >> (j - 1);
         A.dst = static_cast<uint32_t*>((j & 1) ? ctx->fold_a.p : ctx->fold_b.p);
         prev = A.dst;
+      }
+      if (j == tail_j) {  // this round and every later one, in one block
+        if ((rc = ensure(ctx, ctx->tail, sizeof(TailDesc)))) return rc;
+        if (!ctx->tail_host) SC_CUDA(cudaMallocHost(&ctx->tail_host, sizeof(TailDesc)));
+        // the staging is free: every proof ends with a synchronisation of the stream
+        TailDesc& desc = *static_cast<TailDesc*>(ctx->tail_host);
+        std::memset(&desc, 0, sizeof(desc));
+        TailDesc* dev = static_cast<TailDesc*>(ctx->tail.p);
+        desc.r.args = A;
+        desc.r.expr = &dev->e;
+        desc.r.partials = A.partials;
+        desc.r.num_items = 1;
+        desc.r.round_items = 1;
+        desc.r.tail_rounds = n - 1 - j;
+        desc.r.skip1_min_pairs = static_cast<uint32_t>(kSkip1MinPairs);
+        desc.r.fold_a = static_cast<uint32_t*>(ctx->fold_a.p);
+        desc.r.fold_b = static_cast<uint32_t*>(ctx->fold_b.p);
+        desc.e = E;
+        SC_CUDA(cudaMemcpyAsync(dev, &desc, sizeof(desc), cudaMemcpyHostToDevice, ctx->stream));
+        BatchTickArgs T;
+        T.rounds = &dev->r;
+        T.items = nullptr;
+        T.num_items = 1;
+        T.pad = 0;
+        T.head = nullptr;
+        T.tile = A.pairs;
+        cudaEvent_t ev;
+        if ((rc = timing_begin(ctx, &ev))) return rc;
+        if ((rc = batch_kernel_launch(L, K, DMAX, f, 1, tail_threads, tail_smem, ctx->stream, T))) return rc;
+        if ((rc = timing_end(ctx))) return rc;
+        break;
       }
       uint64_t per_block = static_cast<uint64_t>(threads);
       if (use_point_parallel(L) && shape == kShapeGeneric) {  // pairs a block holds: one per lane group
@@ -284,10 +364,11 @@ int sc_ctx_destroy(sc_ctx* ctx) {
   if (!ctx) return SC_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (DevBuf* b : {&ctx->fold_a, &ctx->fold_b, &ctx->partials, &ctx->state})
+  for (DevBuf* b : {&ctx->fold_a, &ctx->fold_b, &ctx->partials, &ctx->state, &ctx->tail})
     if (b->p) cudaFree(b->p);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->host_state) cudaFreeHost(ctx->host_state);
+  if (ctx->tail_host) cudaFreeHost(ctx->tail_host);
   delete ctx;
   return SC_OK;
 }
@@ -591,6 +672,25 @@ int prove_segment(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int n
 }  // namespace sc_host
 
 extern "C" {
+
+int sc_prove_launches(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds, int* out_launches,
+                      int* out_tail_round) {
+  if (!ctx || !field || !expr) return fail(SC_ERR_INVALID, "NULL argument");
+  if (num_rounds < 1 || num_rounds > kMaxRounds)
+    return fail(SC_ERR_INVALID, "num_rounds %d outside 1..%d", num_rounds, kMaxRounds);
+  SC_CUDA(cudaSetDevice(ctx->device));
+  int tail = num_rounds, threads = 0;
+  size_t smem = 0;
+  uint8_t role[16];
+  const int dclass = degree_class(expr->degree);
+  const int shape = dclass == 4 ? match_shape(*expr, role) : kShapeGeneric;
+  const int rc = tail_round(ctx, field->hf.L, field_kind(field->hf.p, field->hf.L), dclass, expr->num_vars, shape,
+                            num_rounds, 0, num_rounds, &tail, &threads, &smem);
+  if (rc) return rc;
+  if (out_launches) *out_launches = tail < num_rounds ? tail + 1 : num_rounds;
+  if (out_tail_round) *out_tail_round = tail;
+  return SC_OK;
+}
 
 int sc_transcript_words(const sc_field* field, const sc_expr* expr, int num_rounds, uint64_t* out_words) {
   if (!field || !expr || !out_words) return fail(SC_ERR_INVALID, "NULL argument");

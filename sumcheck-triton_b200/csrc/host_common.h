@@ -59,11 +59,21 @@ int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigne
 
 using sc_host::DevBuf;
 
+// Launch shape of the batched kernel for one (L, field kind, degree class, tables): the
+// plain path's tail launch (capi.cu) looks it up once per context.
+struct TailShape {
+  int L, kind, dclass, tables, threads;
+  size_t smem;
+};
+
 struct sc_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int sm_count = 0;
   DevBuf fold_a, fold_b, partials, state;
+  DevBuf tail;                        // the tail launch's BatchRound and ExprDev
+  void* tail_host = nullptr;          // pinned staging of the same
+  std::vector<TailShape> tail_shapes;
   uint32_t* host_state = nullptr;  // pinned staging of the proof state
   size_t host_state_bytes = 0;
   // per-launch timing of the round kernels (off by default)

@@ -131,6 +131,7 @@ SIGNATURES = {
     "sc_tables_tag": (c_int, [c_int, POINTER(c_int32), c_uint64, U64P]),
     "sc_prove_resume": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, U32P, c_int, U32P, c_uint64]),
     "sc_server_destroy": (c_int, [c_void_p]),
+    "sc_prove_launches": (c_int, [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_int)]),
     "sc_prove": (
         c_int,
         [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, U32P, U32P, U32P, U32P, U32P, U64P],

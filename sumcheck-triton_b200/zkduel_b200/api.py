@@ -358,6 +358,20 @@ def prove_host(host_tables, expr: CompiledExpression | Expression, spec: FieldSp
     return prove_device(dev, expr, spec, num_rounds, challenge_mode, challenges)
 
 
+def prove_launches(expr: CompiledExpression | Expression, spec: FieldSpec, num_rounds: int,
+                   device=None) -> tuple[int, int]:
+    """(kernel launches, first tail round) of ``prove_device`` for this proof: one launch per
+    round before the tail round, then one for all the rest (``sc_prove_launches``)."""
+    if not isinstance(expr, CompiledExpression):
+        expr = CompiledExpression(encode_expression(expr), spec.modulus)
+    ctx = get_context(device)
+    fld = get_device_field(spec, ctx.device)
+    launches, tail = ctypes.c_int(0), ctypes.c_int(0)
+    _lib.check(_lib.load().sc_prove_launches(ctx.handle, fld.handle, expr.handle, int(num_rounds),
+                                             ctypes.byref(launches), ctypes.byref(tail)), "sc_prove_launches")
+    return launches.value, tail.value
+
+
 def calibrate_imad(ctx: Context | None = None) -> float:
     """Measured 32-bit multiply-add rate of the device (IMAD/s), the integer-pipe peak."""
     ctx = ctx or get_context()
