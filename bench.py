@@ -520,8 +520,10 @@ def main() -> int:
     if roof:
         line["roofline"] = roof
 
-    if rank == 0 and world == 1 and not args.no_e2e:
-        line["e2e"] = e2e_measure(work, args, device, path == "batched", tuning)
+    if not args.no_e2e:  # every rank: its own host buffers and PCIe link, max time over ranks
+        e2e = e2e_measure(work, args, device, path == "batched", tuning, world)
+        if rank == 0:
+            line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0, sample_stride=4)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
@@ -635,19 +637,26 @@ def served_measure(args, device, rank: int, world: int) -> dict:
     return out
 
 
-def e2e_measure(work: Workload, args, device, batched: bool, tuning=None) -> dict:
+def e2e_measure(work: Workload, args, device, batched: bool, tuning=None, world: int = 1) -> dict:
     """Host-buffer path: per step, every proof's canonical tables go from pinned host memory
     to the device and are converted to Montgomery form there; the proofs run (batched, or
-    one sc_prove per proof); every proof's results are read back to the host."""
+    one sc_prove per proof); every proof's results are read back to the host. With several
+    ranks each proves its own stream from its own host buffers; the step time is the
+    slowest rank's, and the bytes and proofs are the whole job's."""
     import torch
 
     from zkduel_b200 import api
     from zkduel_b200.batch import HostBatchProver
 
-    host = []
-    for s, spec, _e, t in work.items:
-        canon = api.download_tables(t, spec)
-        host.append(torch.from_numpy(canon.view("int32")).pin_memory())
+    host, why = [], ""
+    try:
+        for s, spec, _e, t in work.items:
+            canon = api.download_tables(t, spec)
+            host.append(torch.from_numpy(canon.view("int32")).pin_memory())
+    except (RuntimeError, MemoryError) as e:  # pinned host memory is a per-node resource
+        why = f"pinning {len(host)}/{len(work.items)} proofs' tables failed: {str(e)[:160]}"
+    if max_over_ranks(1.0 if why else 0.0, world) > 0:  # every rank takes the same path
+        return {"unavailable": why or "another rank could not pin its host tables"}
     h2d = sum(h.numel() * 4 for h in host)
 
     if batched:
@@ -664,20 +673,21 @@ def e2e_measure(work: Workload, args, device, batched: bool, tuning=None) -> dic
     step()
     torch.cuda.synchronize(device)
     steps = max(1, min(args.steps, 3))
+    barrier(world)
     t0 = time.perf_counter()
     for _ in range(steps):
         res = step()
     torch.cuda.synchronize(device)
-    dt = (time.perf_counter() - t0) / steps
+    dt = max_over_ranks((time.perf_counter() - t0) / steps, world)
     d2h = sum(p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
               for p in res)
     pcie = h2d_bandwidth(device)
-    return {"value": STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": dt * 1e3,
+    return {"value": world * STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": world * h2d,
+            "d2h_bytes_per_step": world * d2h, "ms_per_step": dt * 1e3, "ranks": world,
             "path": (f"batched, {args.e2e_chunks} chunks" if batched else "plain") + " (host buffers)",
             "steps": steps, "timer": "host wall clock around synchronised steps",
             # the bound of this path: the step's host-to-device bytes at the measured copy rate
-            "pcie_h2d_gbs": pcie, "h2d_frac": (h2d / dt / 1e9) / pcie if pcie else None}
+            "pcie_h2d_gbs": pcie, "h2d_frac": (h2d / dt / 1e9) / pcie if pcie else None}  # per rank
 
 
 def h2d_bandwidth(device, nbytes: int = 1 << 30) -> float:
