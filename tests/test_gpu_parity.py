@@ -178,3 +178,27 @@ def test_sumcheck_accepts_short_challenge_list_and_rejects_bad_input():
     with pytest.raises(ValueError, match="Unknown backend"):
         api.sumcheck(tables, q=spec.modulus, expression=expr, challenges=[1, 1], num_rounds=2, backend="reference")
     assert api.available_backends() == ["b200"]
+
+
+def test_tail_launch_plan_and_timings():
+    """Generic expressions: a launch per round up to the tail round, then one launch for the
+    rest (sc_prove_launches), and the per-launch timings come in that number. The
+    compile-time shapes keep a launch per round. Results are pinned by the oracle tests."""
+    for name, tail_expected in (("plain_p32", True), ("plain_goldilocks", False), ("plain_bls", False)):
+        cfg = PLAIN_CONFIGS[name]
+        spec = get_field(cfg.bit_width)
+        n = 14
+        launches, tail = api.prove_launches(cfg.expression, spec, n)
+        if tail_expected:
+            assert 0 < tail < n - 1 and launches == tail + 1
+        else:
+            assert (launches, tail) == (n, n)
+        ctx = api.get_context()
+        ctx.launch_times()  # drop earlier records
+        ctx.set_timing(True)
+        try:
+            api.prove(cfg.expression, cfg.bit_width, n, seed=5, table_kinds=cfg.table_kinds())
+            times = ctx.launch_times()
+        finally:
+            ctx.set_timing(False)
+        assert len(times) == launches and all(t > 0 for t in times)
