@@ -215,6 +215,12 @@ int sc_batch_wait(sc_batch* batch);
 int sc_batch_result(sc_batch* batch, int index, uint32_t* out_round_polys,
                     uint32_t* out_challenges, uint32_t* out_finals, uint32_t* out_claim0,
                     uint64_t* out_checksum);
+/* Outputs of every proof of the last run in one call: proof 0's arrays, then proof 1's, and
+ * so on, each laid out as sc_prove's (out_round_polys holds sum_p n_p (d_p + 1) L words,
+ * out_challenges sum_p n_p L, out_finals sum_p (1 + K_p) L, out_claim0 count x L,
+ * out_checksums count). Any may be NULL. */
+int sc_batch_results(sc_batch* batch, uint32_t* out_round_polys, uint32_t* out_challenges,
+                     uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksums);
 /* A batch splits its proofs by degree class (degree <= 2, <= 4, <= 7); each class runs
  * its own sequence of ticks on its own stream. sc_batch_classes gives each class's degree
  * bound and tick count; sc_batch_class_proofs the indices of its proofs. */

@@ -486,6 +486,25 @@ int sc_batch_result(sc_batch* B, int index, uint32_t* out_round_polys, uint32_t*
   return SC_OK;
 }
 
+int sc_batch_results(sc_batch* B, uint32_t* out_round_polys, uint32_t* out_challenges, uint32_t* out_finals,
+                     uint32_t* out_claim0, uint64_t* out_checksums) {
+  if (!B) return fail(SC_ERR_INVALID, "NULL batch");
+  const int L = B->L;
+  size_t op = 0, oc = 0, of = 0;
+  for (int p = 0; p < B->count; ++p) {
+    const int n = B->n[p], d = B->d[p], K = B->K[p];
+    int rc = sc_batch_result(B, p, out_round_polys ? out_round_polys + op : nullptr,
+                             out_challenges ? out_challenges + oc : nullptr, out_finals ? out_finals + of : nullptr,
+                             out_claim0 ? out_claim0 + static_cast<size_t>(p) * L : nullptr,
+                             out_checksums ? out_checksums + p : nullptr);
+    if (rc) return rc;
+    op += static_cast<size_t>(n) * (d + 1) * L;
+    oc += static_cast<size_t>(n) * L;
+    of += static_cast<size_t>(1 + K) * L;
+  }
+  return SC_OK;
+}
+
 int sc_batch_destroy(sc_batch* B) {
   if (!B) return SC_OK;
   cudaSetDevice(B->ctx->device);

@@ -96,6 +96,7 @@ SIGNATURES = {
     "sc_batch_join": (c_int, [c_void_p]),
     "sc_batch_wait": (c_int, [c_void_p]),
     "sc_batch_result": (c_int, [c_void_p, c_int, U32P, U32P, U32P, U32P, U64P]),
+    "sc_batch_results": (c_int, [c_void_p, U32P, U32P, U32P, U32P, U64P]),
     "sc_batch_tick_times": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), c_int, POINTER(c_int)]),
     "sc_batch_classes": (c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), c_int, POINTER(c_int)]),
     "sc_batch_class_proofs": (c_int, [c_void_p, c_int, POINTER(c_int32), c_int, POINTER(c_int)]),

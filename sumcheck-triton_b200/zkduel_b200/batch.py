@@ -162,7 +162,33 @@ class BatchProver:
         raise IndexError(i)
 
     def results(self) -> list[Proof]:
-        return [self.result(i) for i in range(len(self.items))]
+        """Outputs of every proof of the last run: one native call per field group
+        (``sc_batch_results``), each proof's arrays views into the group's buffers."""
+        out: list[Proof | None] = [None] * len(self.items)
+        lib = _lib.load()
+        p = lambda a: a.ctypes.data_as(_lib.U32P)  # noqa: E731
+        for g in self.groups:
+            L = g.spec.limbs
+            shapes = [(int(self.items[i][2]), e.degree, e.num_vars) for i, e in zip(g.indices, g.exprs)]
+            polys = np.zeros(sum(n * (d + 1) * L for n, d, _k in shapes), dtype=np.uint32)
+            chals = np.zeros(sum(n * L for n, _d, _k in shapes), dtype=np.uint32)
+            finals = np.zeros(sum((1 + k) * L for _n, _d, k in shapes), dtype=np.uint32)
+            claim0 = np.zeros(len(shapes) * L, dtype=np.uint32)
+            cs = np.zeros(len(shapes), dtype=np.uint64)
+            rc = lib.sc_batch_results(g.handle, p(polys), p(chals), p(finals), p(claim0),
+                                      cs.ctypes.data_as(_lib.U64P))
+            _lib.check(rc, "sc_batch_results")
+            op = oc = of = 0
+            for j, (i, e) in enumerate(zip(g.indices, g.exprs)):
+                n, d, k = shapes[j]
+                out[i] = Proof(g.spec, n, d, e.encoded.var_names,
+                               polys[op:op + n * (d + 1) * L].reshape(n, d + 1, L), chals[oc:oc + n * L].reshape(n, L),
+                               finals[of:of + (1 + k) * L].reshape(1 + k, L), claim0[j * L:(j + 1) * L],
+                               int(cs[j]))
+                op += n * (d + 1) * L
+                oc += n * L
+                of += (1 + k) * L
+        return out
 
     def close(self) -> None:
         for g in self.groups:
