@@ -409,13 +409,6 @@ inline StateOffsets state_offsets(int n, int K, int L) {
   return o;
 }
 
-// The batched round kernel's launch shape and launch (instantiated once, in batch.cu):
-// threads per block, grid (resident blocks on every SM) and dynamic shared memory for
-// requests of up to kmax tables.
-int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int sm_count, int* threads, int* grid,
-                       size_t* smem);
-int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
-                        cudaStream_t stream, const BatchTickArgs& T);
 
 // ---- transcripts: a proof stopped at a round boundary, resumable from the same tables
 //
