@@ -228,6 +228,9 @@ class ReplayReport:
             "makespan_s": self.makespan_s,
             "busy_s": self.stats.get("busy_s"),
             "ticks": self.stats.get("ticks"),
+            "worker_build_s": self.stats.get("build_s"),   # composing and issuing ticks
+            "worker_wait_s": self.stats.get("wait_s"),     # blocked on the GPU
+            "worker_alloc_s": self.stats.get("alloc_s"),   # pool allocations at admission
             "peak_inflight": self.stats.get("peak_inflight"),
             "peak_footprint_gb": self.stats.get("peak_footprint", 0) / 1e9,
         }
