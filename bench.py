@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--path", choices=["batched", "plain"], default="batched")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain-configs", action="store_true",
+                    help="skip the three plain configs' latency (GPU) and CPU-port timings")
     ap.add_argument("--e2e-chunks", type=int, default=16,
                     help="host-buffer path: batches whose copies overlap the proving of the ones before")
     ap.add_argument("--no-cpu", action="store_true")
@@ -530,6 +532,8 @@ def main() -> int:
                                 "sample": f"{done} proofs (every 4th of the 512-proof stream), {spent:.1f} s"}
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         line["reference_cuda"] = reference_cuda_compare()
+    if rank == 0 and world == 1 and not args.no_plain_configs:
+        line["plain_configs"] = plain_configs_measure(device, cpu=not args.no_cpu)
     if args.served > 0:
         del batcher, steps_fn, work
         torch.cuda.empty_cache()
@@ -546,6 +550,62 @@ def main() -> int:
 REF_BIN = ROOT / "oracle" / "_ref" / "field_sumcheck_cuda"
 CLI_BIN = ROOT / "sumcheck-triton_b200" / "bin" / "field_sumcheck_b200"
 PLAIN_CASES = (("poly_ab", 16, 32), ("zk_vanilla_zerocheck_hp", 24, 64), ("poly_abcg_plus_deg", 22, 256))
+
+
+def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20) -> dict:
+    """The three plain configs one proof at a time at full size, tables resident: per-proof
+    device time (CUDA events) as p50 / p99 and proofs/s. Beside it the C port of the
+    reference's CPU prover (every host thread) on the same tables: at full size for the
+    32-bit config; for the others at num_vars = cpu_vars, the time scaled by 2^(n - cpu_vars)
+    (the work is linear in the table size), with the GPU checksum compared at that size."""
+    import torch
+
+    from oracle import c_oracle as C
+    from oracle import oracle as O
+    from zkduel_b200 import api
+    from zkduel_b200.configs import PLAIN_CONFIGS
+    from zkduel_b200.fields import get_field
+
+    out = {}
+    for name, cfg in PLAIN_CONFIGS.items():
+        spec = get_field(cfg.bit_width)
+        enc = api.encode_expression(cfg.expression)
+        kinds = [api._lib.SC_TABLE_BERNOULLI if k == "bernoulli" else api._lib.SC_TABLE_UNIFORM
+                 for k in cfg.table_kinds()]
+        expr = api.CompiledExpression(enc, spec.modulus)
+        n = cfg.num_vars
+        t = api.generate_tables(spec, enc.num_vars, n, kinds, cfg.seed, device)
+        for _ in range(3):
+            api.prove_device(t, expr, spec, n, "sha3")
+        reps = 200 if n <= 16 else 40
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            p = api.prove_device(t, expr, spec, n, "sha3")
+            b.record()
+            torch.cuda.synchronize(device)
+            ms.append(a.elapsed_time(b))
+        del t
+        ms.sort()
+        entry = {"num_vars": n, "gpu": {"p50_ms": ms[len(ms) // 2], "p99_ms": ms[min(len(ms) - 1, int(0.99 * len(ms)))],
+                                        "proofs_per_s": 1e3 * len(ms) / sum(ms), "proofs": len(ms),
+                                        "timer": "CUDA events around each prove_device (results on the host)"}}
+        if cpu:
+            nc = n if n <= 16 else cpu_vars
+            terms, k = O.indexed_terms(cfg.expression)
+            ct = C.generate(spec.modulus, spec.limbs, kinds, nc, cfg.seed)
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            res = C.prove(terms, k, spec.modulus, spec.limbs, ct, "sha3", threads=threads)
+            sec = time.perf_counter() - t0
+            gt = api.generate_tables(spec, enc.num_vars, nc, kinds, cfg.seed, device)
+            gp = api.prove_device(gt, expr, spec, nc, "sha3")
+            entry["cpu_port"] = {"ms_per_proof": sec * 1e3 * (1 << (n - nc)), "threads": threads,
+                                 "sample": "full size" if nc == n else f"num_vars {nc}, time x 2^{n - nc}",
+                                 "checksum_equal_gpu": gp.checksum == res["checksum"]}
+        out[name] = entry
+    return out
 
 
 def reference_cuda_compare() -> dict:
