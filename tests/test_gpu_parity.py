@@ -202,3 +202,23 @@ def test_tail_launch_plan_and_timings():
         finally:
             ctx.set_timing(False)
         assert len(times) == launches and all(t > 0 for t in times)
+
+
+@pytest.mark.parametrize("name,bw,n", [("plain_goldilocks", 64, 13), ("plain_goldilocks", 64, 16),
+                                       ("plain_bls", 64, 15), ("plain_bls", 32, 14)])
+def test_shape_kernels_match_c_oracle_at_larger_sizes(name, bw, n):
+    """The compile-time shape kernels on rounds of 2^12 pairs and more (g(1) from the claim,
+    many blocks, grid-stride loops), at 64 and 32 bits; bit-exact against the C oracle."""
+    from oracle import c_oracle as C
+
+    cfg = PLAIN_CONFIGS[name]
+    spec = get_field(bw)
+    kinds = cfg.table_kinds()
+    proof = api.prove(cfg.expression, bw, n, seed=21, table_kinds=kinds)
+    terms, k = O.indexed_terms(cfg.expression)
+    tables = C.generate(spec.modulus, spec.limbs, [1 if x == "bernoulli" else 0 for x in kinds], n, 21)
+    res = C.prove(terms, k, spec.modulus, spec.limbs, tables, "sha3")
+    assert np.array_equal(proof.round_polys_mont, res["round_polys"])
+    assert np.array_equal(proof.challenges_mont, res["challenges"])
+    assert np.array_equal(proof.finals_mont, res["finals"])
+    assert proof.checksum == res["checksum"]
