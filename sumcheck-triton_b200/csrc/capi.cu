@@ -171,7 +171,10 @@ struct ProveRun {
       if (j == tail_j) {  // this round and every later one, in one block
         if ((rc = ensure(ctx, ctx->tail, sizeof(TailDesc)))) return rc;
         if (!ctx->tail_host) SC_CUDA(cudaMallocHost(&ctx->tail_host, sizeof(TailDesc)));
-        // the staging is free: every proof ends with a synchronisation of the stream
+        if (!ctx->tail_copied) SC_CUDA(cudaEventCreateWithFlags(&ctx->tail_copied, cudaEventDisableTiming));
+        // the staging's previous copy has landed (a proof ends with a stream synchronisation,
+        // unless it failed part way)
+        SC_CUDA(cudaEventSynchronize(ctx->tail_copied));
         TailDesc& desc = *static_cast<TailDesc*>(ctx->tail_host);
         std::memset(&desc, 0, sizeof(desc));
         TailDesc* dev = static_cast<TailDesc*>(ctx->tail.p);
@@ -186,6 +189,7 @@ struct ProveRun {
         desc.r.fold_b = static_cast<uint32_t*>(ctx->fold_b.p);
         desc.e = E;
         SC_CUDA(cudaMemcpyAsync(dev, &desc, sizeof(desc), cudaMemcpyHostToDevice, ctx->stream));
+        SC_CUDA(cudaEventRecord(ctx->tail_copied, ctx->stream));
         BatchTickArgs T;
         T.rounds = &dev->r;
         T.items = nullptr;
@@ -369,6 +373,7 @@ int sc_ctx_destroy(sc_ctx* ctx) {
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->host_state) cudaFreeHost(ctx->host_state);
   if (ctx->tail_host) cudaFreeHost(ctx->tail_host);
+  if (ctx->tail_copied) cudaEventDestroy(ctx->tail_copied);
   delete ctx;
   return SC_OK;
 }

@@ -73,6 +73,7 @@ struct sc_ctx {
   DevBuf fold_a, fold_b, partials, state;
   DevBuf tail;                        // the tail launch's BatchRound and ExprDev
   void* tail_host = nullptr;          // pinned staging of the same
+  cudaEvent_t tail_copied = nullptr;  // the staging's last copy to the device
   std::vector<TailShape> tail_shapes;
   uint32_t* host_state = nullptr;  // pinned staging of the proof state
   size_t host_state_bytes = 0;
