@@ -20,8 +20,8 @@ constexpr uint64_t kSkip1MinPairs = uint64_t{1} << 12;
 
 inline bool round_skip1(int n, int j) { return j >= 1 && (uint64_t{1} << (n - j - 1)) >= kSkip1MinPairs; }
 
-// Tail launch: from the first round with at most one pair per thread of the batched kernel's
-// block, that one block proves the rest of the proof (batch_round_kernel's tail rounds: no
+// Tail launch: from the first round with at most a few pairs a thread of the batched kernel's
+// block (tail_round), that one block proves the rest of the proof (batch_round_kernel's tail rounds: no
 // grid-wide partials and no launch per round). Generic expressions only: the batched kernel
 // has no compile-time shapes, and the shape kernels' small rounds beat its generic evaluator.
 // Measured on B200 (median of 10 proofs): a b over 2^32 - 5, n = 16, 0.254 -> 0.228 ms,
@@ -51,15 +51,19 @@ int tail_shape(sc_ctx* ctx, int L, int kind, int dclass, int tables, int* thread
   return SC_OK;
 }
 
-// The round the tail launch starts at (stop: none), for a proof run up to round stop.
+// The round the tail launch starts at (stop: none), for a proof run up to round stop: the
+// first with at most a few pairs a thread of the batched kernel's block.
 int tail_round(sc_ctx* ctx, int L, int kind, int dclass, int tables, int shape, int n, int first, int stop,
                int* out_round, int* threads, size_t* smem) {
   *out_round = stop;
   if (!kPlainTails || stop != n || shape != kShapeGeneric) return SC_OK;
   int rc = tail_shape(ctx, L, kind, dclass, tables, threads, smem);
   if (rc) return rc;
+  // pairs a thread at the tail's first round: measured on B200 (1, 2 or 4), 4 was best for
+  // a b over 2^32 - 5 (n = 16: 0.233 -> 0.224 ms), 1-2 for 4 and 8 limbs (4 was 3-7% slower)
+  const uint64_t per_thread = L == 1 ? 4 : (L <= 4 ? 2 : 1);
   for (int j = first; j < n - 1; ++j)
-    if (((uint64_t{1} << n) >> (j + 1)) <= static_cast<uint64_t>(*threads)) {
+    if (((uint64_t{1} << n) >> (j + 1)) <= static_cast<uint64_t>(*threads) * per_thread) {
       *out_round = j;
       break;
     }
