@@ -302,6 +302,16 @@ def timed(fn, steps: int, world: int, device):
 # ------------------------------------------------------------------------------ CPU port
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_port_sample(budget_s: float, master_seed: int = 0, sample_stride: int = 16, max_proofs: int | None = None):
     """The C oracle with every host thread on proofs 0, stride, 2 stride, ... of the stream
     until ``budget_s`` of proving time is spent. Returns (proofs/s, proofs, seconds, threads)."""
@@ -345,7 +355,7 @@ def reference_arm(args, rank: int, world: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Montgomery)",
         "data": "synthetic", "config": {"workload": WORKLOAD, "proofs_per_step": done,
                                         "sample": f"proofs 0, 16, 32, ... of the 512-proof stream (first {done})"},
-        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"{done} proofs (every 16th of the stream) per step"},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -529,7 +539,8 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, done, spent, threads = cpu_port_sample(budget_s=15.0, sample_stride=4)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
-                                "sample": f"{done} proofs (every 4th of the 512-proof stream), {spent:.1f} s"}
+                                "sample": f"{done} proofs (every 4th of the 512-proof stream), {spent:.1f} s",
+                                "cpu_model": cpu_model()}
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         line["reference_cuda"] = reference_cuda_compare()
     if rank == 0 and world == 1 and not args.no_plain_configs:
