@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--profile-batch", action="store_true",
                     help="profile mode: build the mixed stream (--stream-count proofs), run the batch twice, exit")
     ap.add_argument("--stream-count", type=int, default=STREAM_COUNT, help="proofs in the stream (profile mode)")
+    ap.add_argument("--profile-aux", action="store_true",
+                    help="profile mode: the plain path's generic kernels (point-parallel 8-limb, 2-limb generic, "
+                         "tail launch), a resume refold and a host-table conversion, each twice, then exit")
     return ap.parse_args()
 
 
@@ -372,6 +375,8 @@ def main() -> int:
         return profile_case(args)
     if args.profile_batch:
         return profile_batch(args)
+    if args.profile_aux:
+        return profile_aux(args)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -561,6 +566,35 @@ def main() -> int:
 REF_BIN = ROOT / "oracle" / "_ref" / "field_sumcheck_cuda"
 CLI_BIN = ROOT / "sumcheck-triton_b200" / "bin" / "field_sumcheck_b200"
 PLAIN_CASES = (("poly_ab", 16, 32), ("zk_vanilla_zerocheck_hp", 24, 64), ("poly_abcg_plus_deg", 22, 256))
+
+
+def profile_aux(args) -> int:
+    """Kernels outside the plain configs and the batch, on inputs larger than L2, twice each
+    (the first warms up): a generic 256-bit proof at n = 21 (point-parallel kernel, tail
+    launch), a generic 64-bit proof at n = 22 (generic round kernel), the refold of a 64-bit
+    n = 22 transcript resumed at round 10 (fold_kernel), and the Montgomery conversion of
+    host tables (convert_tables_kernel)."""
+    import torch
+
+    from zkduel_b200 import api
+    from zkduel_b200 import transcript as tr
+    from zkduel_b200.fields import get_field
+
+    f256, f64 = get_field(256), get_field(64)
+    e256 = ((1, ("a", "b")), (3, ("c",)))
+    e64 = ((1, ("a", "b", "c")), (5, ("d",)))
+    t256 = api.generate_tables(f256, 3, 21, [0] * 3, 1)
+    t64 = api.generate_tables(f64, 4, 22, [0] * 4, 2)
+    host = api.download_tables(t64, f64)
+    half = tr.prove_rounds(t64, e64, f64, 10, tr.start(e64, f64, 22))
+    for _ in range(2):
+        api.prove_device(t256, e256, f256, 21, "sha3")
+        api.prove_device(t64, e64, f64, 22, "sha3")
+        tr.prove_rounds(t64, e64, f64, 22, half)
+        api.upload_tables(host, f64)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_aux": True, "bytes_256": t256.numel() * 4, "bytes_64": t64.numel() * 4}))
+    return 0
 
 
 def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20) -> dict:
