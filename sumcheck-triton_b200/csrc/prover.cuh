@@ -576,8 +576,15 @@ constexpr int kPointParallelThreads = 128;
 #ifndef SC_L4_MIN_BLOCKS
 #define SC_L4_MIN_BLOCKS 2
 #endif
+// 2-limb generic and batched kernels at 3 blocks/SM (<= 85 registers; 74-80 used, the
+// degree <= 7 class spills 4-20 bytes): the 512-proof mixed stream went from 9.89k to 10.16k
+// proofs/s (the 64-bit ticks' busy time 31.5 -> 30.0 ms), plain 64-bit proofs the same. At 4
+// limbs, 3 blocks/SM spilled 700+ bytes and served p50 went from 1.03 to 1.31 ms.
+#ifndef SC_L2_MIN_BLOCKS
+#define SC_L2_MIN_BLOCKS 3
+#endif
 __host__ __device__ constexpr int kernel_min_blocks(int L) {
-  return L >= 8 ? SC_L8_MIN_BLOCKS : (L == 4 ? SC_L4_MIN_BLOCKS : 1);
+  return L >= 8 ? SC_L8_MIN_BLOCKS : (L == 4 ? SC_L4_MIN_BLOCKS : (L == 2 ? SC_L2_MIN_BLOCKS : 1));
 }
 #ifndef SC_SHAPE_MIN_BLOCKS
 #define SC_SHAPE_MIN_BLOCKS 2
