@@ -350,7 +350,7 @@ typedef struct sc_server_stats {
   double build_s;              /* worker time composing and issuing ticks */
 } sc_server_stats;
 
-/* threads: 0 = default; pairs_per_thread: 0 = 2 (a tile is threads x pairs_per_thread
+/* threads: 0 = default; pairs_per_thread: 0 = 1 (a tile is threads x pairs_per_thread
  * pairs); chunk_items: tiles per tick for the larger rounds, 0 = two waves of the grid. */
 int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm_budget_bytes,
                      int max_inflight, int max_tables, int threads, int pairs_per_thread,

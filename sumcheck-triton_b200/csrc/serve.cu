@@ -857,10 +857,11 @@ int sc_server_create(int device, const sc_field* field, int policy, uint64_t hbm
   S->budget = hbm_budget_bytes;
   S->max_inflight = max_inflight;
   S->max_tables = max_tables;
-  // default tile: 2 pairs a thread. Measured on B200 over 4,000 requests of the served stream
-  // at 80% load: p50 1.47 ms with 4, 1.24 ms with 2, 1.25 ms with 1 (p90 worse), 1.40 ms with
-  // 3; the tick budget (chunk_items, 0.5-4 waves) changed p50 by under 2%.
-  S->ppt = pairs_per_thread ? pairs_per_thread : 2;
+  // default tile: 1 pair a thread. Measured on B200 over 4,000 requests of the served stream
+  // at 80% load, 4-limb kernels at 2 blocks/SM (p50 / p90 / p99 ms): 1 pair 0.99 / 7.6 / 25.0,
+  // 2 pairs 1.12 / 7.15 / 25.0, 4 pairs 1.40 / 7.15 / 26.1. The tick budget (chunk_items,
+  // 0.5-4 waves) changed p50 by under 2%.
+  S->ppt = pairs_per_thread ? pairs_per_thread : 1;
   S->stats.budget = hbm_budget_bytes;
   S->t0 = Clock::now();
   auto bail = [&](int rc) {
