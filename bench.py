@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--profile-batch", action="store_true",
                     help="profile mode: build the mixed stream (--stream-count proofs), run the batch twice, exit")
     ap.add_argument("--stream-count", type=int, default=STREAM_COUNT, help="proofs in the stream (profile mode)")
+    ap.add_argument("--profile-served", action="store_true",
+                    help="profile mode: a burst of 120 requests of the served stream (num_vars 12..18) through "
+                         "the continuous server, then exit")
     ap.add_argument("--profile-aux", action="store_true",
                     help="profile mode: the plain path's generic kernels (point-parallel 8-limb, 2-limb generic, "
                          "tail launch), a resume refold and a host-table conversion, each twice, then exit")
@@ -377,6 +380,8 @@ def main() -> int:
         return profile_batch(args)
     if args.profile_aux:
         return profile_aux(args)
+    if args.profile_served:
+        return profile_served(args)
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -566,6 +571,21 @@ def main() -> int:
 REF_BIN = ROOT / "oracle" / "_ref" / "field_sumcheck_cuda"
 CLI_BIN = ROOT / "sumcheck-triton_b200" / "bin" / "field_sumcheck_b200"
 PLAIN_CASES = (("poly_ab", 16, 32), ("zk_vanilla_zerocheck_hp", 24, 64), ("poly_abcg_plus_deg", 22, 256))
+
+
+def profile_served(args) -> int:
+    """A burst of served requests (2^127 - 1, num_vars 12..18, degree 3-7) through the
+    continuous server: its ticks (4-limb batched kernel), tail rounds, lane launches and
+    table generation."""
+    from zkduel_b200.fields import get_field
+    from zkduel_b200.serve import ProofServer, replay
+    from zkduel_b200.streams import served_stream
+
+    reqs = served_stream(120, rate_per_s=1e9, seed=5, min_vars=12, max_vars=18)
+    with ProofServer(get_field(128)) as srv:
+        rep, _ = replay(srv, reqs)
+    print(json.dumps({"profile_served": len(reqs), "p50_ms": rep.summary()["p50_ms"]}))
+    return 0
 
 
 def profile_aux(args) -> int:
