@@ -49,10 +49,11 @@ struct DevBuf {
 
 // The batched round kernel's launch shape and launch (instantiated once, in batch.cu):
 // threads per block, grid (resident blocks on every SM) and dynamic shared memory for
-// requests of up to kmax tables.
-int batch_kernel_setup(int L, int K, int dclass, int kmax, int threads_req, int sm_count, int* threads, int* grid,
+// requests of up to kmax tables. dmax is the largest degree the instance proves: a degree
+// class (2, 4, 7) or 6.
+int batch_kernel_setup(int L, int K, int dmax, int kmax, int threads_req, int sm_count, int* threads, int* grid,
                        size_t* smem);
-int batch_kernel_launch(int L, int K, int dclass, const sc_field* field, unsigned grid, int threads, size_t smem,
+int batch_kernel_launch(int L, int K, int dmax, const sc_field* field, unsigned grid, int threads, size_t smem,
                         cudaStream_t stream, const BatchTickArgs& T);
 
 }  // namespace sc_host
