@@ -241,6 +241,11 @@ def profiled_traffic_ratio(L: int):
     return float(m.group(1)) if m else None
 
 
+def all_ranks_ok(ok: bool, world: int) -> bool:
+    """True on every rank when every rank passes ok (one collective, the same on all ranks)."""
+    return max_over_ranks(0.0 if ok else 1.0, world) == 0.0
+
+
 def sum_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
@@ -780,7 +785,7 @@ def e2e_measure(work: Workload, args, device, batched: bool, tuning=None, world:
             host.append(torch.from_numpy(canon.view("int32")).pin_memory())
     except (RuntimeError, MemoryError) as e:  # pinned host memory is a per-node resource
         why = f"pinning {len(host)}/{len(work.items)} proofs' tables failed: {str(e)[:160]}"
-    if max_over_ranks(1.0 if why else 0.0, world) > 0:  # every rank takes the same path
+    if not all_ranks_ok(not why, world):  # every rank takes the same path
         return {"unavailable": why or "another rank could not pin its host tables"}
     h2d = sum(h.numel() * 4 for h in host)
 

@@ -45,6 +45,9 @@ def _worker(rank: int, world: int, port: int, out):
         "sum": bench.sum_over_ranks(1.5 * (rank + 1), w),
         "stream_seeds": [s.seed for s in batched_stream(8, rank)],
         "reference_arm": bench.reference_arm(None, rank, w) if rank != 0 else None,
+        # e2e: if one rank cannot pin its host tables, every rank skips the measurement
+        "all_ok": bench.all_ranks_ok(True, w),
+        "one_fails": bench.all_ranks_ok(rank != 1, w),
     }
     bench.barrier(w)
     dist.destroy_process_group()
@@ -61,3 +64,5 @@ def test_two_ranks_reduce_and_split_the_stream():
     assert res[0]["sum"] == res[1]["sum"] == 4.5  # throughput: every rank's proofs
     assert res[0]["stream_seeds"] != res[1]["stream_seeds"]  # replicas prove different proofs
     assert res[1]["reference_arm"] == 0  # non-zero ranks do no reference work
+    assert res[0]["all_ok"] and res[1]["all_ok"]
+    assert not res[0]["one_fails"] and not res[1]["one_fails"]  # both ranks skip together
