@@ -65,7 +65,7 @@ def test_split_proof_over_two_processes():
     from zkduel_b200.fields import get_field
 
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork after CUDA is up in this process
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
