@@ -53,6 +53,8 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 SERVED_COUNT = 20000
 SERVED_LOAD = 0.8
 SERVED_BUDGET = 150 * 10**9
+CPU_SAMPLE_STRIDE = 16
+CPU_SAMPLE_PROOFS = STREAM_COUNT // CPU_SAMPLE_STRIDE  # proofs 0, 16, ..., 496 of the stream
 
 
 def parse():
@@ -68,6 +70,8 @@ def parse():
     ap.add_argument("--e2e-chunks", type=int, default=16,
                     help="host-buffer path: batches whose copies overlap the proving of the ones before")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE_PROOFS,
+                    help="proofs in the fixed CPU sample (every 16th proof of the stream, from proof 0)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuned ones")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference CUDA executable comparison")
     ap.add_argument("--served", type=int, default=SERVED_COUNT,
@@ -191,10 +195,36 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def relaunch_ranks(n_gpus: int) -> int | None:
+    """One process per GPU. Under a launcher (WORLD_SIZE set) the world must be --gpus;
+    without one, --gpus N > 1 re-runs this command under torch.distributed.run with N ranks
+    on this node and returns its exit code. None: go on in this process."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != n_gpus:
+            print(json.dumps({"error": f"--gpus {n_gpus} but WORLD_SIZE={world}: launch one rank per GPU"}),
+                  flush=True)
+            return 2
+        return None
+    if n_gpus <= 1:
+        return None
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n_gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def dist_setup(n_gpus: int):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n_gpus:
+        raise SystemExit(f"--gpus {n_gpus} but WORLD_SIZE={world}")
     if world > 1:
         import datetime
 
@@ -323,17 +353,19 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def cpu_port_sample(budget_s: float, master_seed: int = 0, sample_stride: int = 16, max_proofs: int | None = None):
-    """The C oracle with every host thread on proofs 0, stride, 2 stride, ... of the stream
-    until ``budget_s`` of proving time is spent. Returns (proofs/s, proofs, seconds, threads)."""
+def cpu_port_sample(proofs: int = CPU_SAMPLE_PROOFS, master_seed: int = 0):
+    """The C oracle with every host thread on a fixed sample of the stream: proofs 0, 16,
+    32, ... (the first ``proofs`` of them; all 32 by default), the same proofs every run.
+    Table generation is outside the timed region, as it is for the GPU. Returns
+    (proofs/s, proofs, seconds, threads)."""
     from oracle import c_oracle as C
     from oracle import oracle as O
     from zkduel_b200.fields import get_field
     from zkduel_b200.streams import batched_stream
 
     threads = os.cpu_count() or 1
-    specs = batched_stream(STREAM_COUNT, master_seed)[::sample_stride]
-    done, spent = 0, 0.0
+    specs = batched_stream(STREAM_COUNT, master_seed)[::CPU_SAMPLE_STRIDE][:max(1, proofs)]
+    spent = 0.0
     for s in specs:
         f = get_field(s.bit_width)
         terms, k = O.indexed_terms(s.expression)
@@ -341,33 +373,35 @@ def cpu_port_sample(budget_s: float, master_seed: int = 0, sample_stride: int = 
         t0 = time.perf_counter()
         C.prove(terms, k, f.modulus, f.limbs, t, "sha3", threads=threads)
         spent += time.perf_counter() - t0
-        done += 1
-        if spent >= budget_s or (max_proofs and done >= max_proofs):
-            break
-    return done / spent, done, spent, threads
+    return len(specs) / spent, len(specs), spent, threads
+
+
+def cpu_sample_text(done: int) -> str:
+    return (f"proofs 0, {CPU_SAMPLE_STRIDE}, {2 * CPU_SAMPLE_STRIDE}, ... ({done} proofs, every "
+            f"{CPU_SAMPLE_STRIDE}th of the 512-proof stream, master seed 0), the same every run")
 
 
 def reference_arm(args, rank: int, world: int):
+    """The reference's CPU prover path, restated in C (the reference's own prover is pure
+    Python and its source does not travel with this repository), on every host thread.
+    A step proves the fixed sample once; rank 0 alone runs it."""
     if rank != 0:
         return 0
     per_step = []
-    info = None
+    done, threads = 0, 1
     for i in range(args.warmup + args.steps):
-        rate, done, spent, threads = cpu_port_sample(budget_s=8.0, max_proofs=12)
-        info = (done, threads)
+        rate, done, spent, threads = cpu_port_sample(args.cpu_sample)
         if i >= args.warmup:
-            per_step.append(done / rate)
+            per_step.append(spent)
     total = sum(per_step)
-    done, threads = info
     value = done * len(per_step) / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(per_step),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Montgomery)",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "proofs_per_step": done,
-                                        "sample": f"proofs 0, 16, 32, ... of the 512-proof stream (first {done})"},
+        "data": "synthetic", "config": {"workload": WORKLOAD, "proofs_per_step": done, "sample": cpu_sample_text(done)},
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
-                         "sample": f"{done} proofs (every 16th of the stream) per step"},
+                         "sample": cpu_sample_text(done)},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -387,6 +421,9 @@ def main() -> int:
         return profile_aux(args)
     if args.profile_served:
         return profile_served(args)
+    rc = relaunch_ranks(args.gpus)
+    if rc is not None:
+        return rc
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -548,14 +585,14 @@ def main() -> int:
         line["roofline"] = roof
 
     if not args.no_e2e:  # every rank: its own host buffers and PCIe link, max time over ranks
-        e2e = e2e_measure(work, args, device, path == "batched", tuning, world)
+        resident = batcher.results() if path == "batched" else run_plain(work)
+        e2e = e2e_measure(work, args, device, path == "batched", tuning, world, expect=resident)
         if rank == 0:
             line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, done, spent, threads = cpu_port_sample(budget_s=15.0, sample_stride=4)
+        rate, done, spent, threads = cpu_port_sample(args.cpu_sample)
         line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
-                                "sample": f"{done} proofs (every 4th of the 512-proof stream), {spent:.1f} s",
-                                "cpu_model": cpu_model()}
+                                "sample": f"{cpu_sample_text(done)}; {spent:.1f} s", "cpu_model": cpu_model()}
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         line["reference_cuda"] = reference_cuda_compare()
     if rank == 0 and world == 1 and not args.no_plain_configs:
@@ -767,12 +804,14 @@ def served_measure(args, device, rank: int, world: int) -> dict:
     return out
 
 
-def e2e_measure(work: Workload, args, device, batched: bool, tuning=None, world: int = 1) -> dict:
+def e2e_measure(work: Workload, args, device, batched: bool, tuning=None, world: int = 1, expect=None) -> dict:
     """Host-buffer path: per step, every proof's canonical tables go from pinned host memory
     to the device and are converted to Montgomery form there; the proofs run (batched, or
     one sc_prove per proof); every proof's results are read back to the host. With several
     ranks each proves its own stream from its own host buffers; the step time is the
-    slowest rank's, and the bytes and proofs are the whole job's."""
+    slowest rank's, and the bytes and proofs are the whole job's. ``expect``: the resident
+    path's proofs; the last timed step's proofs must equal them (round polynomials,
+    challenges, final values, checksum) or the measurement is reported unavailable."""
     import torch
 
     from zkduel_b200 import api
@@ -811,13 +850,25 @@ def e2e_measure(work: Workload, args, device, batched: bool, tuning=None, world:
     dt = max_over_ranks((time.perf_counter() - t0) / steps, world)
     d2h = sum(p.round_polys_mont.nbytes + p.challenges_mont.nbytes + p.finals_mont.nbytes + p.claim0_mont.nbytes + 8
               for p in res)
+    import numpy as np
+
+    bad = [] if expect is None else [
+        i for i, (a, b) in enumerate(zip(res, expect))
+        if not (a.checksum == b.checksum and np.array_equal(a.round_polys_mont, b.round_polys_mont)
+                and np.array_equal(a.challenges_mont, b.challenges_mont) and np.array_equal(a.finals_mont, b.finals_mont))]
+    if expect is not None and len(res) != len(expect):
+        bad.append(-1)
+    if not all_ranks_ok(not bad, world):
+        return {"unavailable": f"host-buffer proofs differ from the resident path's (proofs {bad[:8]})"
+                if bad else "another rank's host-buffer proofs differ from its resident path's"}
     pcie = h2d_bandwidth(device)
     return {"value": world * STREAM_COUNT / dt, "unit": "proofs/s", "h2d_bytes_per_step": world * h2d,
             "d2h_bytes_per_step": world * d2h, "ms_per_step": dt * 1e3, "ranks": world,
             "path": (f"batched, {args.e2e_chunks} chunks" if batched else "plain") + " (host buffers)",
             "steps": steps, "timer": "host wall clock around synchronised steps",
             # the bound of this path: the step's host-to-device bytes at the measured copy rate
-            "pcie_h2d_gbs": pcie, "h2d_frac": (h2d / dt / 1e9) / pcie if pcie else None}  # per rank
+            "pcie_h2d_gbs": pcie, "h2d_frac": (h2d / dt / 1e9) / pcie if pcie else None,  # per rank
+            "results_equal_resident": expect is not None}
 
 
 def h2d_bandwidth(device, nbytes: int = 1 << 30) -> float:

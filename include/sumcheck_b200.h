@@ -167,8 +167,10 @@ int sc_prove_launches(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, i
  * the library holds until exit; proofs needing more (about K L 2^n 3 bytes of fold
  * buffers plus under 1 MiB) fail with SC_ERR_UNSUPPORTED before anything runs. The first
  * call on a device looks up that array's device address: make it before any stream
- * capture. Calls share the array: calls that overlap on one GPU race, so issue them on
- * one stream or one after another. */
+ * capture, and do not reset the device's primary context (cudaDeviceReset) after it.
+ * Synchronous: returns once the results are in the caller's arrays. Calls share the
+ * array: calls that overlap on one GPU race, so issue them on one stream or one after
+ * another. */
 int sc_prove_noalloc(sc_ctx* ctx, const sc_field* field, const sc_expr* expr, int num_rounds,
                      const uint32_t* tables_dev, int challenge_mode,
                      const uint32_t* explicit_challenges, uint32_t* out_round_polys,

@@ -30,6 +30,11 @@ def load():
     lib.oracle_prove.argtypes = [c_int, POINTER(c_uint32), c_int, c_int, POINTER(c_int64), POINTER(c_int32),
                                  POINTER(c_int32), POINTER(c_int32), c_int, c_void_p, c_int, POINTER(c_uint32),
                                  c_int, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_uint64)]
+    lib.oracle_prove_seeded.restype = c_int
+    lib.oracle_prove_seeded.argtypes = [c_int, POINTER(c_uint32), c_int, c_int, POINTER(c_int64), POINTER(c_int32),
+                                        POINTER(c_int32), POINTER(c_int32), c_int, POINTER(c_int32), c_uint64, c_int,
+                                        POINTER(c_uint32), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        POINTER(c_uint64)]
     lib.oracle_generate.restype = c_int
     lib.oracle_generate.argtypes = [c_int, POINTER(c_uint32), c_int, c_int, POINTER(c_int32), c_uint64, c_void_p]
     lib.oracle_sha3_256.restype = None
@@ -63,19 +68,19 @@ def sha3_256(data: bytes) -> bytes:
     return bytes(out)
 
 
-def prove(terms, num_tables: int, p: int, L: int, tables: np.ndarray, mode: str = "sha3",
-          explicit=None, threads: int | None = None) -> dict:
-    """Outputs as Montgomery limb arrays: round_polys (n, d+1, L), challenges (n, L),
-    finals (1+K, L), claim0 (L,), checksum int."""
-    K = num_tables
-    n = int(tables.shape[2]).bit_length() - 1
-    d = max(len(f) for _c, f in terms)
+def _encode_terms(terms):
     coeffs = [int(c) for c, _f in terms]
     lens = [len(f) for _c, f in terms]
     offs, flat = [], []
     for _c, f in terms:
         offs.append(len(flat))
         flat.extend(f)
+    return ((c_int64 * len(coeffs))(*coeffs), (c_int32 * len(lens))(*lens), (c_int32 * len(offs))(*offs),
+            (c_int32 * max(1, len(flat)))(*flat), max(lens))
+
+
+def _run(call, terms, K: int, p: int, L: int, n: int, mode: str, explicit, threads):
+    coeffs, lens, offs, flat, d = _encode_terms(terms)
     polys = np.zeros((n, d + 1, L), dtype=np.uint32)
     chals = np.zeros((n, L), dtype=np.uint32)
     finals = np.zeros((1 + K, L), dtype=np.uint32)
@@ -83,13 +88,35 @@ def prove(terms, num_tables: int, p: int, L: int, tables: np.ndarray, mode: str 
     cs = c_uint64(0)
     m = {"sha3": 0, "fixed": 1, "explicit": 2}[mode]
     ex = _u32([w for c in (explicit or [0] * n) for w in _limbs(int(c) % p, L)])
-    t = np.ascontiguousarray(tables, dtype=np.uint32)
     threads = threads or os.cpu_count() or 1
-    rc = load().oracle_prove(L, _u32(_limbs(p, L)), K, len(terms), (c_int64 * len(coeffs))(*coeffs),
-                             (c_int32 * len(lens))(*lens), (c_int32 * len(offs))(*offs),
-                             (c_int32 * max(1, len(flat)))(*flat), n, t.ctypes.data_as(c_void_p), m, ex,
-                             int(threads), polys.ctypes.data_as(c_void_p), chals.ctypes.data_as(c_void_p),
-                             finals.ctypes.data_as(c_void_p), claim0.ctypes.data_as(c_void_p), ctypes.byref(cs))
+    rc = call(coeffs, lens, offs, flat, m, ex, int(threads), polys.ctypes.data_as(c_void_p),
+              chals.ctypes.data_as(c_void_p), finals.ctypes.data_as(c_void_p), claim0.ctypes.data_as(c_void_p),
+              ctypes.byref(cs))
     if rc:
-        raise RuntimeError(f"oracle_prove failed ({rc})")
+        raise RuntimeError(f"oracle prove failed ({rc})")
     return {"round_polys": polys, "challenges": chals, "finals": finals, "claim0": claim0, "checksum": int(cs.value)}
+
+
+def prove(terms, num_tables: int, p: int, L: int, tables: np.ndarray, mode: str = "sha3",
+          explicit=None, threads: int | None = None) -> dict:
+    """Outputs as Montgomery limb arrays: round_polys (n, d+1, L), challenges (n, L),
+    finals (1+K, L), claim0 (L,), checksum int."""
+    K = num_tables
+    n = int(tables.shape[2]).bit_length() - 1
+    t = np.ascontiguousarray(tables, dtype=np.uint32)
+    return _run(lambda co, le, of, fl, m, ex, th, *out:
+                load().oracle_prove(L, _u32(_limbs(p, L)), K, len(terms), co, le, of, fl, n,
+                                    t.ctypes.data_as(c_void_p), m, ex, th, *out),
+                terms, K, p, L, n, mode, explicit, threads)
+
+
+def prove_seeded(terms, num_tables: int, p: int, L: int, n: int, kinds, seed: int, mode: str = "sha3",
+                 explicit=None, threads: int | None = None) -> dict:
+    """``prove`` of the tables ``generate(p, L, kinds, n, seed)`` would return, without
+    holding them: round 0 generates its entries on the fly, so a proof of 2^n entries per
+    table needs host memory for 2^(n-1) (Montgomery) entries per table only."""
+    K = num_tables
+    return _run(lambda co, le, of, fl, m, ex, th, *out:
+                load().oracle_prove_seeded(L, _u32(_limbs(p, L)), K, len(terms), co, le, of, fl, n,
+                                           (c_int32 * K)(*kinds), c_uint64(seed & (2**64 - 1)), m, ex, th, *out),
+                terms, K, p, L, n, mode, explicit, threads)

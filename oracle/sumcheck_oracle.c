@@ -224,47 +224,73 @@ static uint64_t mix(uint64_t x) {
   return z ^ (z >> 31);
 }
 
-/* Canonical tables, limb-planar (K, L, 2^n): kinds 0 uniform, 1 bernoulli, 2 + v arith. */
-int oracle_generate(int L, const uint32_t* p, int K, int n, const int32_t* kinds, uint64_t seed, uint32_t* out) {
-  const uint64_t N = (uint64_t)1 << n;
+/* What the generators need of a modulus: its bit mask per limb and, when p < 2^64, p. */
+typedef struct {
+  int L;
+  uint32_t p[MAXL];
+  uint32_t mask[MAXL];
+  uint64_t p64;
+  uint64_t seed;
+} gen_t;
+
+static void gen_setup(gen_t* g, int L, const uint32_t* p, uint64_t seed) {
+  memset(g, 0, sizeof(*g));
+  g->L = L;
+  memcpy(g->p, p, 4 * L);
+  g->seed = seed;
   int bits = 0;
   for (int l = L - 1; l >= 0 && !bits; --l)
     if (p[l]) bits = 32 * l + (32 - __builtin_clz(p[l]));
-  uint32_t mask[MAXL];
   for (int l = 0; l < L; ++l) {
     int lo = 32 * l;
-    mask[l] = bits >= lo + 32 ? 0xFFFFFFFFu : (bits <= lo ? 0u : ((1u << (bits - lo)) - 1u));
+    g->mask[l] = bits >= lo + 32 ? 0xFFFFFFFFu : (bits <= lo ? 0u : ((1u << (bits - lo)) - 1u));
   }
   int fits64 = 1;
   for (int l = 2; l < L; ++l) fits64 = fits64 && p[l] == 0;
-  uint64_t p64 = fits64 ? (((uint64_t)(L > 1 ? p[1] : 0)) << 32) | p[0] : 0;
+  g->p64 = fits64 ? (((uint64_t)(L > 1 ? p[1] : 0)) << 32) | p[0] : 0;
+}
+
+static uint64_t gen_key(const gen_t* g, int k) { return mix(g->seed ^ mix((uint64_t)k + 0x632BE59BD9B4E019ULL)); }
+
+/* Entry i of table k (canonical limbs): kind 0 uniform, 1 bernoulli, 2 + v arith. */
+static void gen_entry(const gen_t* g, const field_t* f, int kind, uint64_t key, uint64_t i, uint32_t* x) {
+  const int L = g->L;
+  memset(x, 0, 4 * MAXL);
+  if (kind == 0) {
+    int ok = 0;
+    for (int a = 0; a < 64 && !ok; ++a) {
+      for (int w = 0; w < (L + 1) / 2; ++w) {
+        uint64_t z = mix(key + ((i << 8) | (uint64_t)((a << 2) | w)));
+        x[2 * w] = (uint32_t)z;
+        if (2 * w + 1 < L) x[2 * w + 1] = (uint32_t)(z >> 32);
+      }
+      for (int l = 0; l < L; ++l) x[l] &= g->mask[l];
+      ok = !geq(f, x, g->p);
+    }
+    if (!ok) sub_raw(L, x, g->p, x);
+  } else if (kind == 1) {
+    x[0] = (uint32_t)mix(key + (i << 8)) & 1u;
+  } else {
+    uint64_t v = (uint64_t)(kind - 2);
+    uint64_t s = (g->seed & 0xFFFFFFFFULL) + 7919ULL * (v + 1) + 104729ULL * (i + 1);
+    if (g->p64) s %= g->p64;
+    x[0] = (uint32_t)s;
+    if (L > 1) x[1] = (uint32_t)(s >> 32);
+  }
+}
+
+/* Canonical tables, limb-planar (K, L, 2^n): kinds 0 uniform, 1 bernoulli, 2 + v arith. */
+int oracle_generate(int L, const uint32_t* p, int K, int n, const int32_t* kinds, uint64_t seed, uint32_t* out) {
+  const uint64_t N = (uint64_t)1 << n;
   field_t f;
   field_setup(&f, L, p);
+  gen_t g;
+  gen_setup(&g, L, p, seed);
   for (int k = 0; k < K; ++k) {
-    uint64_t key = mix(seed ^ mix((uint64_t)k + 0x632BE59BD9B4E019ULL));
+    const uint64_t key = gen_key(&g, k);
     for (uint64_t i = 0; i < N; ++i) {
-      uint32_t x[MAXL] = {0};
-      if (kinds[k] == 0) {
-        int ok = 0;
-        for (int a = 0; a < 64 && !ok; ++a) {
-          for (int w = 0; w < (L + 1) / 2; ++w) {
-            uint64_t z = mix(key + ((i << 8) | (uint64_t)((a << 2) | w)));
-            x[2 * w] = (uint32_t)z;
-            if (2 * w + 1 < L) x[2 * w + 1] = (uint32_t)(z >> 32);
-          }
-          for (int l = 0; l < L; ++l) x[l] &= mask[l];
-          ok = !geq(&f, x, p);
-        }
-        if (!ok) sub_raw(L, x, p, x);
-      } else if (kinds[k] == 1) {
-        x[0] = (uint32_t)mix(key + (i << 8)) & 1u;
-      } else {
-        uint64_t v = (uint64_t)(kinds[k] - 2);
-        uint64_t s = (seed & 0xFFFFFFFFULL) + 7919ULL * (v + 1) + 104729ULL * (i + 1);
-        if (p64) s %= p64;
-        x[0] = (uint32_t)s;
-        if (L > 1) x[1] = (uint32_t)(s >> 32);
-      }
+      uint32_t x[MAXL];
+      gen_entry(&g, &f, kinds[k], key, i, x);
       for (int l = 0; l < L; ++l) out[((uint64_t)k * L + l) * N + i] = x[l];
     }
   }
@@ -280,8 +306,11 @@ typedef struct {
   const int32_t* offs;
   const int32_t* flat;
   const uint32_t* cm; /* T x L Montgomery coefficients */
-  const uint32_t* cur; /* K x N x L element-major, Montgomery */
+  const uint32_t* cur; /* K x N x L element-major, Montgomery (NULL: generate, see gen) */
   uint32_t* nxt;
+  const gen_t* gen;    /* round 0 of a seeded proof: entries generated on the fly */
+  const int32_t* kinds;
+  uint64_t keys[MAXK];
   uint64_t N;          /* entries per table in cur */
   uint64_t lo, hi;     /* pair range */
   uint32_t r[MAXL];
@@ -289,16 +318,29 @@ typedef struct {
   int phase; /* 0 eval, 1 fold */
 } job_t;
 
+/* Entries 2i and 2i + 1 of table k, Montgomery, into e[0..2L). */
+static const uint32_t* pair_at(const job_t* J, int k, uint64_t i, uint32_t* buf) {
+  const int L = J->f->L;
+  if (J->cur) return J->cur + ((uint64_t)k * J->N + 2 * i) * L;
+  for (int h = 0; h < 2; ++h) {
+    uint32_t x[MAXL];
+    gen_entry(J->gen, J->f, J->kinds[k], J->keys[k], 2 * i + h, x);
+    f_mul(J->f, x, J->f->r2, buf + h * L);
+  }
+  return buf;
+}
+
 static void* run_job(void* arg) {
   job_t* J = (job_t*)arg;
   const field_t* f = J->f;
   const int L = f->L, K = J->K;
+  uint32_t buf[2 * MAXL];
   if (J->phase == 0) {
     uint32_t v[MAXK][MAXL], df[MAXK][MAXL];
     memset(J->acc, 0, sizeof(J->acc));
     for (uint64_t i = J->lo; i < J->hi; ++i) {
       for (int k = 0; k < K; ++k) {
-        const uint32_t* e = J->cur + ((uint64_t)k * J->N + 2 * i) * L;
+        const uint32_t* e = pair_at(J, k, i, buf);
         memcpy(v[k], e, 4 * L);
         f_sub(f, e + L, e, df[k]);
       }
@@ -319,7 +361,7 @@ static void* run_job(void* arg) {
     const uint64_t half = J->N / 2;
     for (int k = 0; k < K; ++k)
       for (uint64_t i = J->lo; i < J->hi; ++i) {
-        const uint32_t* e = J->cur + ((uint64_t)k * J->N + 2 * i) * L;
+        const uint32_t* e = pair_at(J, k, i, buf);
         uint32_t d[MAXL], x[MAXL];
         f_sub(f, e + L, e, d);
         f_mul(f, J->r, d, x);
@@ -347,34 +389,50 @@ static void run_parallel(job_t* jobs, int threads, uint64_t count) {
 }
 
 /*
- * tables: canonical, limb-planar (K, L, 2^n). mode 0 sha3, 1 fixed (r = 1), 2 explicit
- * (explicit_canon: n x L canonical limbs). Outputs in Montgomery limbs:
- *   out_polys n x (d + 1) x L, out_chals n x L, out_finals (1 + K) x L, out_claim0 L.
+ * tables: canonical, limb-planar (K, L, 2^n); or NULL, and then round 0 generates every
+ * entry on the fly from (kinds, seed) -- the same values oracle_generate writes -- so a
+ * seeded proof holds only the folded tables (half the entries, Montgomery). mode 0 sha3,
+ * 1 fixed (r = 1), 2 explicit (explicit_canon: n x L canonical limbs). Outputs in
+ * Montgomery limbs: out_polys n x (d + 1) x L, out_chals n x L, out_finals (1 + K) x L,
+ * out_claim0 L.
  */
-int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, const int32_t* lens,
-                 const int32_t* offs, const int32_t* flat, int n, const uint32_t* tables, int mode,
-                 const uint32_t* explicit_canon, int threads, uint32_t* out_polys, uint32_t* out_chals,
-                 uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum) {
+static int prove_core(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, const int32_t* lens,
+                      const int32_t* offs, const int32_t* flat, int n, const uint32_t* tables,
+                      const int32_t* kinds, uint64_t seed, int mode, const uint32_t* explicit_canon, int threads,
+                      uint32_t* out_polys, uint32_t* out_chals, uint32_t* out_finals, uint32_t* out_claim0,
+                      uint64_t* out_checksum) {
   if (threads < 1) threads = 1;
   if (threads > 256) threads = 256;
-  if (K > MAXK || L > MAXL || n < 1) return 1;
+  if (K > MAXK || L > MAXL || n < 1 || n > 40) return 1;
   field_t f;
   field_setup(&f, L, p);
+  gen_t g;
+  gen_setup(&g, L, p, seed);
   int d = 0;
   for (int m = 0; m < T; ++m) d = lens[m] > d ? lens[m] : d;
   if (d > MAXP - 1) return 1;
   uint64_t N = (uint64_t)1 << n;
-  uint32_t* cur = (uint32_t*)malloc(sizeof(uint32_t) * K * N * L);
-  uint32_t* nxt = (uint32_t*)malloc(sizeof(uint32_t) * K * (N / 2 > 0 ? N / 2 : 1) * L);
+  const uint64_t sizeA = tables ? N : N / 2, sizeB = tables ? N / 2 : (N / 4 > 0 ? N / 4 : 1);
+  uint32_t* bufA = (uint32_t*)malloc(sizeof(uint32_t) * K * sizeA * L);
+  uint32_t* bufB = (uint32_t*)malloc(sizeof(uint32_t) * K * sizeB * L);
   uint32_t* cm = (uint32_t*)malloc(sizeof(uint32_t) * T * L);
   job_t* jobs = (job_t*)calloc(threads, sizeof(job_t));
-  if (!cur || !nxt || !cm || !jobs) return 2;
-  for (int k = 0; k < K; ++k)
-    for (uint64_t i = 0; i < N; ++i) {
-      uint32_t x[MAXL];
-      for (int l = 0; l < L; ++l) x[l] = tables[((uint64_t)k * L + l) * N + i];
-      f_mul(&f, x, f.r2, cur + ((uint64_t)k * N + i) * L);
-    }
+  if (!bufA || !bufB || !cm || !jobs) {
+    free(bufA);
+    free(bufB);
+    free(cm);
+    free(jobs);
+    return 2;
+  }
+  uint32_t* cur = tables ? bufA : NULL;
+  uint32_t* nxt = tables ? bufB : bufA;
+  if (tables)
+    for (int k = 0; k < K; ++k)
+      for (uint64_t i = 0; i < N; ++i) {
+        uint32_t x[MAXL];
+        for (int l = 0; l < L; ++l) x[l] = tables[((uint64_t)k * L + l) * N + i];
+        f_mul(&f, x, f.r2, cur + ((uint64_t)k * N + i) * L);
+      }
   for (int m = 0; m < T; ++m) {
     int64_t c = coeffs[m];
     uint64_t mag = c < 0 ? (uint64_t)(-(c + 1)) + 1 : (uint64_t)c;
@@ -402,6 +460,9 @@ int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, 
       J->nxt = nxt;
       J->N = N;
       J->phase = 0;
+      J->gen = &g;
+      J->kinds = kinds;
+      for (int k = 0; k < K && !cur; ++k) J->keys[k] = gen_key(&g, k);
       memset(J->acc, 0, sizeof(J->acc)); /* a job with an empty range contributes zero */
     }
     run_parallel(jobs, half < (uint64_t)threads ? 1 : threads, half);
@@ -455,9 +516,14 @@ int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, 
       memcpy(jobs[t].r, r, 4 * L);
     }
     run_parallel(jobs, half < (uint64_t)threads ? 1 : threads, half);
-    uint32_t* tmp = cur;
-    cur = nxt;
-    nxt = tmp;
+    if (cur == NULL) { /* round 0 of a seeded proof: T_1 is in bufA, fold into bufB next */
+      cur = bufA;
+      nxt = bufB;
+    } else {
+      uint32_t* tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
     N = half;
     if (j == n - 1) {
       /* final claim: Lagrange interpolation of g at r; folded values f_k(r) */
@@ -491,9 +557,29 @@ int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, 
     }
   }
   *out_checksum = checksum;
-  free(cur);
-  free(nxt);
+  free(bufA);
+  free(bufB);
   free(cm);
   free(jobs);
   return 0;
+}
+
+int oracle_prove(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, const int32_t* lens,
+                 const int32_t* offs, const int32_t* flat, int n, const uint32_t* tables, int mode,
+                 const uint32_t* explicit_canon, int threads, uint32_t* out_polys, uint32_t* out_chals,
+                 uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum) {
+  if (!tables) return 1;
+  return prove_core(L, p, K, T, coeffs, lens, offs, flat, n, tables, NULL, 0, mode, explicit_canon, threads,
+                    out_polys, out_chals, out_finals, out_claim0, out_checksum);
+}
+
+/* The proof of the seeded tables oracle_generate(L, p, K, n, kinds, seed) would write,
+ * without writing them: round 0 generates its entries on the fly (see prove_core). */
+int oracle_prove_seeded(int L, const uint32_t* p, int K, int T, const int64_t* coeffs, const int32_t* lens,
+                        const int32_t* offs, const int32_t* flat, int n, const int32_t* kinds, uint64_t seed,
+                        int mode, const uint32_t* explicit_canon, int threads, uint32_t* out_polys,
+                        uint32_t* out_chals, uint32_t* out_finals, uint32_t* out_claim0, uint64_t* out_checksum) {
+  if (!kinds) return 1;
+  return prove_core(L, p, K, T, coeffs, lens, offs, flat, n, NULL, kinds, seed, mode, explicit_canon, threads,
+                    out_polys, out_chals, out_finals, out_claim0, out_checksum);
 }

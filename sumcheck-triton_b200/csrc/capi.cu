@@ -160,6 +160,13 @@ struct ProveRun {
       A.pairs = N >> (j + 1);
       A.skip1 = round_skip1(n, j) ? 1 : 0;
       A.want_claim = (j + 1 < n && round_skip1(n, j + 1)) ? 1 : 0;
+      // The first round of a resumed segment whose recorded claim is defined (the round
+      // would take g(1) from it) evaluates g(1) from the tables instead and checks
+      // g(0) + g(1) against that claim: tables other than the ones the recorded rounds were
+      // proved on, or an altered claim, fail with kStatusClaim. Equal values either way, so
+      // the proof is unchanged.
+      A.check_claim = (state_io && j == first && A.skip1) ? 1 : 0;
+      if (A.check_claim) A.skip1 = 0;
       if (j == 0) {
         A.fold = 0;
         A.src = tables;

@@ -14,11 +14,15 @@
 //
 // In host code the array's name stands in for the device object, it is not a device
 // address: the first call on each device (with that device current) asks the runtime for
-// the address with cudaGetSymbolAddress and caches it. Make that first call before any
-// stream capture. All calls share the one array and it keeps the last call's contents;
-// what must start at zero (the proof state's counter and checksum) is cleared by every
-// call. Two calls whose work overlaps on the same GPU race on the array: issue them on one
-// stream, or wait for one before starting the next.
+// the address with cudaGetSymbolAddress and caches it, and sets the round kernels'
+// attributes. Make that first call before any stream capture. The cached address belongs
+// to the device's primary context: do not reset that context (cudaDeviceReset) after the
+// first call on the device, or later calls would launch into an unmapped address.
+// The call is synchronous: it returns once the results are in the caller's arrays.
+// All calls share the one array and it keeps the last call's contents; what must start at
+// zero (the proof state's counter, status and checksum) is cleared by every call. Two
+// calls whose work overlaps on the same GPU race on the array: issue them on one stream,
+// or wait for one before starting the next.
 #include <mutex>
 
 #include "host_common.h"

@@ -87,6 +87,14 @@ __host__ __device__ constexpr int shape_tables(int shape) {
   return shape == kShapeZerocheck ? 9 : (shape == kShapeAbcg ? 6 : 0);
 }
 
+// Device-detected errors, or-ed into ProofState::status (the host fails the call with
+// SC_ERR_DEVICE when it reads a nonzero status):
+//   kStatusClaim  a round that evaluated g(1) directly and was given a claim to meet
+//                 (RoundArgs::check_claim) found g_j(0) + g_j(1) != the claim -- the tables
+//                 are not the ones the recorded rounds were proved on, or the recorded claim
+//                 was altered (a resumed transcript's first round checks this).
+constexpr uint32_t kStatusClaim = 1u;
+
 // Per-proof device state, all Montgomery limbs (written by the finalisation).
 struct ProofState {
   uint32_t* counter;     // block tickets of the running round, reset to 0 after each round
@@ -95,7 +103,7 @@ struct ProofState {
   uint32_t* chals;       // [n][L]
   uint32_t* finals;      // [1 + K][L]: g_{n-1}(r_{n-1}), then f_k(r) for every table
   uint32_t* claim0;      // [L]
-  uint32_t* status;      // nonzero on a device-detected error
+  uint32_t* status;      // nonzero on a device-detected error: kStatusClaim
   uint32_t* claim;       // [L]: g_{j-1}(r_{j-1}), the claim round j's g(0) + g(1) must meet
 };
 
@@ -115,6 +123,8 @@ struct RoundArgs {
   ProofState st;
   uint32_t* ext_out;     // non-null: the round's sums g_j(0..d) go here and the round is not
                          // finalised (one rank of a split proof; the commit finalises it)
+  int32_t check_claim;   // with skip1 == 0: check g_j(0) + g_j(1) against st.claim (kStatusClaim)
+  int32_t pad;
 };
 
 template <int L>
@@ -473,10 +483,17 @@ __device__ void finalize_round(const RoundArgs& A, const ExprDev& E, const Field
   const int d = E.degree;
   const int j = A.round;
   const FieldConsts& fc = *A.fc;
-  // 0. g(1) from the claim this round must meet
+  // 0. g(1) from the claim this round must meet, or, when asked, that claim checked
   if (A.skip1) {
     if (lane == 0) st_fe<L>(g_sm + L, fe_sub(ld_fe_cg<L>(A.st.claim), ld_fe<L>(g_sm), F));
     __syncwarp();
+  } else if (A.check_claim && lane == 0) {
+    const Fe<L> s = fe_add(ld_fe<L>(g_sm), ld_fe<L>(g_sm + L), F);
+    const Fe<L> c = ld_fe_cg<L>(A.st.claim);
+    bool eq = true;
+#pragma unroll
+    for (int l = 0; l < L; ++l) eq = eq && s.w[l] == c.w[l];
+    if (!eq) atomicOr(A.st.status, kStatusClaim);
   }
   // 1. round polynomial and checksum
   for (int i = lane; i < (d + 1) * L; i += 32) A.st.polys[(j * kMaxPoints + i / L) * L + i % L] = g_sm[i];
@@ -798,6 +815,7 @@ __global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
         A.fold = 1;
         A.skip1 = A.pairs >= R.skip1_min_pairs ? 1 : 0;
         A.want_claim = (j + 1 < A.num_rounds && (A.pairs >> 1) >= R.skip1_min_pairs) ? 1 : 0;
+        A.check_claim = 0;
       }
       __syncthreads();
     }

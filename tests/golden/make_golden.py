@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (it is read, never modified):
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <reference checkout>
 
 It writes three files; the tests only read them:
 
@@ -163,7 +163,7 @@ def ref_vars(expr):
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--reference", type=Path, required=True, help="the reference checkout")
     args = ap.parse_args()
     sys.path.insert(0, str(args.reference / "src"))
     import zkduel._expr as ref_expr

@@ -38,8 +38,12 @@ def assert_proof_equals_oracle(proof, res, spec):
     assert len(polys[0][0]) == L
 
 
-def check_transcript_and_identities(proof, terms, spec, mode="sha3"):
-    """Size-independent checks of a proof of any size (verifier side, on the host)."""
+def check_transcript_and_identities(proof, terms, spec, mode="sha3", final_values=None):
+    """Size-independent checks of a proof of any size (verifier side, on the host).
+
+    ``final_values``: f_k(r) recomputed on the host from the tables with the proof's
+    challenges. The final-claim identity is then checked on those, not on the prover's own
+    folded values, so a consistent proof of the wrong tables fails it."""
     p, L = spec.modulus, spec.limbs
     g = proof.round_polys
     ch = proof.challenges
@@ -55,6 +59,9 @@ def check_transcript_and_identities(proof, terms, spec, mode="sha3"):
             assert (row[0] + row[1]) % p == O.lagrange_eval(g[j - 1], ch[j - 1], p), f"round {j} identity"
     assert (g[0][0] + g[0][1]) % p == proof.claim0
     assert O.lagrange_eval(g[-1], ch[-1], p) == proof.final_claim
-    assert O.evaluate_terms(terms, proof.final_values, p) == proof.final_claim
+    if final_values is not None:
+        assert list(final_values) == proof.final_values, "f_k(r) differs from the tables' own"
+    values = proof.final_values if final_values is None else final_values
+    assert O.evaluate_terms(terms, values, p) == proof.final_claim
     assert cs == proof.checksum
     assert all(from_limbs(list(map(int, v))) < p for row in proof.round_polys_mont for v in row)

@@ -63,3 +63,20 @@ def test_c_prove_thread_count_invariant():
     a = C.prove(terms, k, f.modulus, f.limbs, t, threads=1)
     b = C.prove(terms, k, f.modulus, f.limbs, t, threads=7)
     assert np.array_equal(a["round_polys"], b["round_polys"]) and a["checksum"] == b["checksum"]
+
+
+@pytest.mark.parametrize("mode", ["sha3", "explicit"])
+@pytest.mark.parametrize("workload,bw,n,kinds", [
+    ("poly_ab", 32, 1, [0, 0]), ("poly_ab", 32, 9, [0, 1]), ("vanilla_zerocheck_hp", 64, 7, None),
+    ("poly_abcg_plus_deg", 256, 5, None), ("poly_abc", 128, 6, [2 + 3, 0, 1])])
+def test_seeded_prove_equals_table_prove(workload, bw, n, kinds, mode):
+    """Round 0 generating its entries on the fly gives the proof of the generated tables."""
+    f = get_field(bw)
+    terms, k = O.indexed_terms(WORKLOADS[workload])
+    kinds = kinds or [0] * k
+    ch = [random.Random(n + 1).randrange(f.modulus) for _ in range(n)] if mode == "explicit" else None
+    want = C.prove(terms, k, f.modulus, f.limbs, C.generate(f.modulus, f.limbs, kinds, n, 31), mode, ch, threads=2)
+    got = C.prove_seeded(terms, k, f.modulus, f.limbs, n, kinds, 31, mode, ch, threads=3)
+    for key in ("round_polys", "challenges", "finals", "claim0"):
+        assert np.array_equal(got[key], want[key]), key
+    assert got["checksum"] == want["checksum"]

@@ -141,17 +141,58 @@ def test_multi_block_sizes_match_oracle(name):
     assert_proof_equals_oracle(proof, res, spec)
 
 
+def _kind_codes(kinds):
+    return [1 if x == "bernoulli" else 0 for x in kinds]
+
+
 @pytest.mark.parametrize("name", ["plain_p32", "plain_goldilocks", "plain_bls"])
-def test_full_size_config_properties(name):
-    """Full-size workloads: SHA3 transcript, round identities, final claim, determinism."""
+def test_full_size_config_matches_c_oracle(name):
+    """Each plain configuration at its full size (n = 16 / 24 / 22), bit-exact against the C
+    oracle: round polynomials, challenges, final claim and every f_k(r), claim0, checksum.
+    Then the verifier-side identities, with f_k(r) taken from the oracle's fold of the
+    tables (not from the proof), and determinism over two runs."""
+    from oracle import c_oracle as C
+
     cfg = PLAIN_CONFIGS[name]
     spec = get_field(cfg.bit_width)
-    terms, _k = O.indexed_terms(cfg.expression)
+    terms, k = O.indexed_terms(cfg.expression)
     a = api.prove(cfg.expression, cfg.bit_width, cfg.num_vars, cfg.seed, table_kinds=cfg.table_kinds())
-    check_transcript_and_identities(a, terms, spec)
+    res = C.prove_seeded(terms, k, spec.modulus, spec.limbs, cfg.num_vars, _kind_codes(cfg.table_kinds()), cfg.seed)
+    assert np.array_equal(a.round_polys_mont, res["round_polys"])
+    assert np.array_equal(a.challenges_mont, res["challenges"])
+    assert np.array_equal(a.finals_mont, res["finals"])
+    assert np.array_equal(a.claim0_mont, res["claim0"])
+    assert a.checksum == res["checksum"]
+    host_finals = [spec.decode_limbs([int(x) for x in v]) for v in res["finals"][1:]]
+    check_transcript_and_identities(a, terms, spec, final_values=host_finals)
     b = api.prove(cfg.expression, cfg.bit_width, cfg.num_vars, cfg.seed, table_kinds=cfg.table_kinds())
     assert np.array_equal(a.round_polys_mont, b.round_polys_mont) and a.checksum == b.checksum
     assert np.array_equal(a.finals_mont, b.finals_mont)
+
+
+def test_tables_past_2_31_entries_match_c_oracle():
+    """a * b over 2^32 - 5 at n = 31: 2^31 entries per table, so table 1's plane starts at
+    entry 2^31 and the last index of every plane is 2^31 - 1. 32-bit indexing past 2^31
+    elements was the reference's one recorded bug (fixed by size_t indexing,
+    cuda/src/field_sumcheck.cu:596,618). Everything is compared with the C oracle, which
+    generates round 0's entries on the fly (host memory for the folded half only)."""
+    from oracle import c_oracle as C
+
+    n, seed = 31, 7
+    expr = WORKLOADS["poly_ab"]
+    spec = get_field(32)
+    terms, k = O.indexed_terms(expr)
+    free, _total = torch.cuda.mem_get_info()
+    need = 2 * (1 << n) * 4 * 7 // 4  # tables + fold buffers
+    if free < need + (4 << 30):
+        pytest.skip(f"needs {need / 2**30:.0f} GiB of device memory")
+    proof = api.prove(expr, 32, n, seed, table_kinds=["uniform", "uniform"])
+    torch.cuda.empty_cache()
+    res = C.prove_seeded(terms, k, spec.modulus, spec.limbs, n, [0, 0], seed)
+    assert np.array_equal(proof.round_polys_mont, res["round_polys"])
+    assert np.array_equal(proof.challenges_mont, res["challenges"])
+    assert np.array_equal(proof.finals_mont, res["finals"])
+    assert proof.checksum == res["checksum"]
 
 
 def test_plain_p32_full_size_matches_oracle():

@@ -210,3 +210,29 @@ def test_suspend_queued_requests_and_errors():
             _same(srv.result(rid), _alone(spec, e, n, s))
             with pytest.raises(ValueError, match="not suspended"):
                 srv.transcript(rid)
+
+
+@pytest.mark.parametrize("bw,expr,n,j", [
+    (64, ((1, ("x", "y")),), 16, 2),          # generic 2-limb kernel
+    (64, ZEROCHECK, 14, 1),                   # compile-time zerocheck shape
+    (256, ((1, ("a", "b")), (3, ("c",))), 14, 1),  # point-parallel 8-limb kernel
+])
+def test_resume_checks_the_recorded_claim_against_the_tables(bw, expr, n, j):
+    """A resumed segment whose first round would take g(1) from the recorded claim instead
+    evaluates g(1) and checks g(0) + g(1) against that claim on the device: the untouched
+    transcript resumes to the whole proof; an altered claim, or tables other than the ones
+    the recorded rounds were proved on, fail with the device status (kStatusClaim = 1)."""
+    spec = get_field(bw)
+    t, _ = _tables(spec, expr, n, 900 + n)
+    whole = api.prove_device(t, expr, spec, n, "sha3")
+    a = tr.prove_rounds(t, expr, spec, j, tr.start(expr, spec, n))
+    _same(tr.result(tr.prove_rounds(t, expr, spec, n, a), expr, spec), whole)
+    bad = a.words.copy()
+    bad[-spec.limbs] ^= 1  # the claim is the transcript's last L words
+    with pytest.raises(_lib.SumcheckError, match="device status 1"):
+        tr.prove_rounds(t, expr, spec, n, tr.Transcript(bad))
+    other, _ = _tables(spec, expr, n, 901 + n)
+    with pytest.raises(_lib.SumcheckError, match="device status 1"):
+        tr.prove_rounds(other, expr, spec, n, a)
+    # the context proves normally afterwards
+    _same(api.prove_device(t, expr, spec, n, "sha3"), whole)

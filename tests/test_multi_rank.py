@@ -66,3 +66,33 @@ def test_two_ranks_reduce_and_split_the_stream():
     assert res[1]["reference_arm"] == 0  # non-zero ranks do no reference work
     assert res[0]["all_ok"] and res[1]["all_ok"]
     assert not res[0]["one_fails"] and not res[1]["one_fails"]  # both ranks skip together
+
+
+def _bench(args, **env_extra):
+    import json
+    import subprocess
+
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_PORT")}
+    env.update(CUDA_VISIBLE_DEVICES="", **env_extra)
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py")] + args, capture_output=True, text=True,
+                         timeout=600, env=env, cwd=str(ROOT))
+    lines = [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+    return out.returncode, lines, out.stderr
+
+
+def test_bench_gpus_2_launches_two_ranks():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself (torch.distributed.run,
+    gloo here); rank 0 prints the one line, reporting both ranks."""
+    rc, lines, err = _bench(["--gpus", "2", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                             "--cpu-sample", "1"])
+    assert rc == 0, err[-2000:]
+    assert len(lines) == 1, lines
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+
+
+def test_bench_rejects_gpus_other_than_world_size():
+    """Under a launcher, a world size other than --gpus is an error, never a silent
+    run on fewer GPUs."""
+    rc, lines, _err = _bench(["--gpus", "4", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+                             WORLD_SIZE="2", RANK="0", LOCAL_RANK="0")
+    assert rc == 2 and lines and "error" in lines[0]

@@ -43,16 +43,29 @@ def _noalloc(ctx, fld, expr, n, tables, mode, L, d, K, explicit=None):
     return rc, polys, chals, finals, claim0, int(cs.value)
 
 
-CASES = [("plain_goldilocks", 12, "sha3"), ("plain_bls", 10, "sha3"), ("plain_p32", 15, "fixed"),
-         ("plain_goldilocks", 1, "sha3")]
+# (bit width, expression, table kinds, num_vars, challenge mode)
+DEG7 = [["a", "b", "c", "d", "e", "f", "g"], (5, ["a", "h"]), (-1, ["c", "d", "e"])]
+CASES = [
+    (64, PLAIN_CONFIGS["plain_goldilocks"].expression, PLAIN_CONFIGS["plain_goldilocks"].table_kinds(), 12, "sha3"),
+    (256, PLAIN_CONFIGS["plain_bls"].expression, None, 10, "sha3"),
+    (32, PLAIN_CONFIGS["plain_p32"].expression, None, 15, "fixed"),
+    (64, PLAIN_CONFIGS["plain_goldilocks"].expression, PLAIN_CONFIGS["plain_goldilocks"].table_kinds(), 1, "sha3"),
+    (128, [["a", "b", "c"], (3, ["d"])], None, 14, "sha3"),   # 2^127 - 1: the Mersenne product
+    (64, DEG7, None, 9, "sha3"),                              # the degree <= 7 kernel class
+    (256, DEG7, None, 7, "sha3"),
+    # the largest 1-limb proof of 10 tables that fits: fold buffers of 10 x 3 x 2^18 words
+    # (30 MiB) end 2 MiB short of the 32 MiB array, so the carve's last offsets are in use
+    (32, [["t0", "t1"], ["t2", "t3", "t4"], ["t5"], ["t6", "t7"], ["t8", "t9"]], None, 20, "sha3"),
+]
 
 
-@pytest.mark.parametrize("name,n,mode", CASES, ids=[f"{c}-n{n}-{m}" for c, n, m in CASES])
-def test_noalloc_matches_sc_prove_on_two_calls_in_a_row(name, n, mode):
-    cfg = PLAIN_CONFIGS[name]
-    spec = get_field(cfg.bit_width)
-    enc = encode_expression(cfg.expression)
-    kinds = [_lib.SC_TABLE_BERNOULLI if k == "bernoulli" else _lib.SC_TABLE_UNIFORM for k in cfg.table_kinds()]
+@pytest.mark.parametrize("bw,expr_src,kinds,n,mode", CASES,
+                         ids=[f"{bw}-n{n}-{m}-{i}" for i, (bw, _e, _k, n, m) in enumerate(CASES)])
+def test_noalloc_matches_sc_prove_on_two_calls_in_a_row(bw, expr_src, kinds, n, mode):
+    spec = get_field(bw)
+    enc = encode_expression(expr_src)
+    kinds = [_lib.SC_TABLE_BERNOULLI if k == "bernoulli" else _lib.SC_TABLE_UNIFORM
+             for k in (kinds or ["uniform"] * enc.num_vars)]
     tables = api.generate_tables(spec, enc.num_vars, n, kinds, seed=77)
     expr = api.CompiledExpression(enc, spec.modulus)
     ref = api.prove_device(tables, expr, spec, n, mode)  # the existing entry point, sc_prove
@@ -87,6 +100,18 @@ def test_noalloc_explicit_challenges_match_sc_prove():
         assert rc == _lib.SC_OK, _lib.last_error()
         assert np.array_equal(polys, ref.round_polys_mont) and np.array_equal(finals, ref.finals_mont)
         assert cs == ref.checksum
+
+
+def test_noalloc_rejects_one_table_more_than_the_largest_fit():
+    """The largest-fit case above with an 11th table needs 33 MiB: rejected, nothing runs."""
+    spec = get_field(32)
+    enc = encode_expression([["t0", "t1"], ["t2", "t3", "t4"], ["t5"], ["t6", "t7"], ["t8", "t9", "t10"]])
+    expr = api.CompiledExpression(enc, spec.modulus)
+    small = api.generate_tables(spec, enc.num_vars, 4, [0] * enc.num_vars, seed=1)
+    ctx = api.get_context(small.device)
+    fld = api.get_device_field(spec, ctx.device)
+    rc, *_ = _noalloc(ctx, fld, expr, 20, small, "sha3", spec.limbs, enc.degree, enc.num_vars)
+    assert rc == _lib.SC_ERR_UNSUPPORTED and "scratch" in _lib.last_error()
 
 
 def test_noalloc_rejects_proofs_beyond_its_scratch():
