@@ -53,6 +53,8 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 SERVED_COUNT = 20000
 SERVED_LOAD = 0.8
 SERVED_BUDGET = 150 * 10**9
+CAPACITY_MULTIPLES = (1.0, 1.5, 2.0, 3.0, 4.0)  # offered rate / FIFO-plain capacity (1 / E[service])
+CAPACITY_P99_MS = 100.0  # a rate is sustained when throughput >= 95% of it and p99 stays under this
 CPU_SAMPLE_STRIDE = 16
 CPU_SAMPLE_PROOFS = STREAM_COUNT // CPU_SAMPLE_STRIDE  # proofs 0, 16, ..., 496 of the stream
 
@@ -76,6 +78,10 @@ def parse():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference CUDA executable comparison")
     ap.add_argument("--served", type=int, default=SERVED_COUNT,
                     help="requests in the served stream (0: skip the served measurement)")
+    ap.add_argument("--capacity-requests", type=int, default=3000,
+                    help="served capacity: requests per offered rate (0: skip the capacity sweep)")
+    ap.add_argument("--budget-requests", type=int, default=300,
+                    help="served: a burst of requests with num_vars up to 26, where the HBM budget binds (0: skip)")
     ap.add_argument("--case", default=None,
                     help="profile mode: prove one plain config (plain_p32|plain_goldilocks|plain_bls) twice and exit")
     ap.add_argument("--case-vars", type=int, default=None, help="num_vars for --case (default: the config's)")
@@ -353,18 +359,30 @@ def cpu_model() -> str:
     return "unknown"
 
 
+def cpu_sample_specs(proofs: int = CPU_SAMPLE_PROOFS, master_seed: int = 0):
+    """A fixed, stratified sample of the stream: the proofs sorted by (field width,
+    num_vars, index), then every 16th of that order from the 8th on -- so each size class of
+    the stream is represented in proportion and the sample holds about 1/16 of the stream's
+    work (the work of a proof grows as 2^num_vars, so an unsorted every-16th sample is
+    dominated by whichever few large proofs it happens to hit)."""
+    from zkduel_b200.streams import batched_stream
+
+    specs = sorted(batched_stream(STREAM_COUNT, master_seed), key=lambda s: (s.bit_width, s.num_vars, s.index))
+    return specs[CPU_SAMPLE_STRIDE // 2::CPU_SAMPLE_STRIDE][:max(1, proofs)]
+
+
 def cpu_port_sample(proofs: int = CPU_SAMPLE_PROOFS, master_seed: int = 0):
-    """The C oracle with every host thread on a fixed sample of the stream: proofs 0, 16,
-    32, ... (the first ``proofs`` of them; all 32 by default), the same proofs every run.
-    Table generation is outside the timed region, as it is for the GPU. Returns
-    (proofs/s, proofs, seconds, threads)."""
+    """The C oracle with every host thread on the fixed stratified sample
+    (``cpu_sample_specs``), the same proofs every run. Table generation is outside the
+    timed region, as it is for the GPU. Returns (proofs/s, proofs, seconds, threads): with
+    the whole sample (1/16 of the stream's proofs and about 1/16 of its work), proofs/s
+    estimates the rate over the whole stream."""
     from oracle import c_oracle as C
     from oracle import oracle as O
     from zkduel_b200.fields import get_field
-    from zkduel_b200.streams import batched_stream
 
     threads = os.cpu_count() or 1
-    specs = batched_stream(STREAM_COUNT, master_seed)[::CPU_SAMPLE_STRIDE][:max(1, proofs)]
+    specs = cpu_sample_specs(proofs, master_seed)
     spent = 0.0
     for s in specs:
         f = get_field(s.bit_width)
@@ -377,8 +395,9 @@ def cpu_port_sample(proofs: int = CPU_SAMPLE_PROOFS, master_seed: int = 0):
 
 
 def cpu_sample_text(done: int) -> str:
-    return (f"proofs 0, {CPU_SAMPLE_STRIDE}, {2 * CPU_SAMPLE_STRIDE}, ... ({done} proofs, every "
-            f"{CPU_SAMPLE_STRIDE}th of the 512-proof stream, master seed 0), the same every run")
+    return (f"{done} proofs: the 512-proof stream (master seed 0) sorted by (field, num_vars), every "
+            f"{CPU_SAMPLE_STRIDE}th from the {CPU_SAMPLE_STRIDE // 2}th (stratified, about 1/{CPU_SAMPLE_STRIDE} "
+            f"of the stream's work), the same every run")
 
 
 def reference_arm(args, rank: int, world: int):
@@ -800,7 +819,81 @@ def served_measure(args, device, rank: int, world: int) -> dict:
     c, f = out["continuous"], out["fifo_plain"]
     out["p50_speedup_vs_fifo"] = f["p50_ms"] / c["p50_ms"]
     out["p99_speedup_vs_fifo"] = f["p99_ms"] / c["p99_ms"]
+    if args.capacity_requests > 0:
+        out["capacity"] = served_capacity(args, spec, dev, service_s, rank, world)
+    if args.budget_requests > 0:
+        out["budget_binding"] = served_budget_binding(args, spec, dev, device, rank, world)
     torch.cuda.synchronize(device)
+    return out
+
+
+def served_capacity(args, spec, dev: int, service_s: float, rank: int, world: int) -> dict:
+    """Offered load beyond what FIFO-plain can serve: the served distribution replayed at
+    CAPACITY_MULTIPLES x FIFO-plain's capacity (1 / E[plain service]) through both policies,
+    and once as a burst (every request at time 0: the policy's saturated throughput). A
+    rate is sustained when the throughput keeps up with it (>= 95%) and p99 stays under
+    CAPACITY_P99_MS; each policy's capacity is the highest sustained rate."""
+    from zkduel_b200.serve import ProofServer, replay
+    from zkduel_b200.streams import served_stream
+
+    fifo_cap = 1.0 / service_s
+    out = {"fifo_capacity_per_s": fifo_cap, "requests_per_point": args.capacity_requests,
+           "p99_bound_ms": CAPACITY_P99_MS, "rule": "sustained: proofs/s >= 0.95 x offered and p99 <= bound"}
+    for pol in ("continuous", "fifo_plain"):
+        pts = []
+        with ProofServer(spec, policy=pol, budget_bytes=SERVED_BUDGET, device=dev) as srv:
+            srv.reserve(32 << 30)
+            replay(srv, served_stream(50, rate_per_s=1e9, seed=97))
+            for mult in CAPACITY_MULTIPLES:
+                rate = mult * fifo_cap
+                rep, _ = replay(srv, served_stream(args.capacity_requests, rate_per_s=rate,
+                                                   seed=700 + int(10 * mult) + 100 * rank))
+                s = rep.summary()
+                pts.append({"offered_x_fifo": mult, "offered_per_s": rate, "proofs_per_s": s["proofs_per_s"],
+                            "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"]})
+            rep, _ = replay(srv, served_stream(args.capacity_requests, rate_per_s=1e9, seed=799 + 100 * rank))
+        ok = [p["offered_per_s"] for p in pts
+              if p["proofs_per_s"] >= 0.95 * p["offered_per_s"] and p["p99_ms"] <= CAPACITY_P99_MS]
+        entry = {"points": pts, "sustained_per_s": max(ok) if ok else 0.0, "burst_proofs_per_s": rep.proofs_per_s}
+        if world > 1:
+            entry["sustained_per_s"] = sum_over_ranks(entry["sustained_per_s"], world)
+            entry["burst_proofs_per_s"] = sum_over_ranks(entry["burst_proofs_per_s"], world)
+        out[pol] = entry
+    c, f = out["continuous"], out["fifo_plain"]
+    out["sustained_ratio_vs_fifo"] = c["sustained_per_s"] / f["sustained_per_s"] if f["sustained_per_s"] else None
+    out["burst_ratio_vs_fifo"] = c["burst_proofs_per_s"] / f["burst_proofs_per_s"]
+    return out
+
+
+def served_budget_binding(args, spec, dev: int, device, rank: int, world: int) -> dict:
+    """A burst of the served distribution with num_vars up to 26 (up to ~15 GB a request)
+    through the continuous server: the requests' footprints add up to more than the
+    150 GB budget, so admission holds requests back. Reports throughput, latency, the peak
+    admitted footprint (never above the budget) and one large proof checked bit-exact
+    against proving it alone."""
+    from zkduel_b200 import api
+    from zkduel_b200.serve import ProofServer, replay
+    from zkduel_b200.streams import served_stream
+
+    reqs = served_stream(args.budget_requests, rate_per_s=1e9, seed=900 + rank, max_vars=26)
+    big = max(range(len(reqs)), key=lambda i: reqs[i].spec.num_vars)
+    with ProofServer(spec, policy="continuous", budget_bytes=SERVED_BUDGET, device=dev) as srv:
+        fp = sum(srv.footprint(r.spec.expression, r.spec.num_vars) for r in reqs)
+        rep, kept = replay(srv, reqs, keep_results={big})
+    s = rep.summary()
+    sb = reqs[big].spec
+    t = api.generate_tables(spec, sb.num_tables, sb.num_vars, [0] * sb.num_tables, sb.seed, device)
+    alone = api.prove_device(t, sb.expression, spec, sb.num_vars, "sha3")
+    del t
+    got = kept[big]
+    exact = bool(got.checksum == alone.checksum and (got.round_polys_mont == alone.round_polys_mont).all())
+    out = {"requests": len(reqs), "max_num_vars": max(r.spec.num_vars for r in reqs),
+           "sum_footprints_gb": fp / 1e9, "budget_gb": SERVED_BUDGET / 1e9,
+           "peak_footprint_gb": s["peak_footprint_gb"], "proofs_per_s": s["proofs_per_s"], "p50_ms": s["p50_ms"],
+           "p99_ms": s["p99_ms"], "makespan_s": s["makespan_s"], "largest_bit_exact": exact,
+           "largest_num_vars": sb.num_vars}
+    if not exact:
+        raise AssertionError("budget-bound served proof differs from the proof alone")
     return out
 
 

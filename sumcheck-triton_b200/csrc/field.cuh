@@ -137,9 +137,20 @@ __device__ __forceinline__ void gold_mul(uint32_t (&r)[2], const uint32_t (&x32)
 // first; out of line, the 256-bit proofs ran 20-25% faster, the 4-limb served stream ~3%).
 // From SC_OUTLINE_MIN_LIMBS limbs up the product is one out-of-line function, operands and
 // result passed by value in registers.
+#ifndef SC_MUL_EO
+#define SC_MUL_EO 0
+#endif
 template <int L>
 __device__ __noinline__ Fe<L> cios_mul_call(const Fe<L> a, const Fe<L> b, const FieldParams<L, kFieldGeneric> F) {
   Fe<L> r;
+#if SC_MUL_EO
+  if constexpr (L >= 4) {
+    if (F.p[L - 1] < 0x80000000u) {  // p < 2^(32L - 1): the even/odd-chain product applies
+      ptx_mont_mul_eo<L>(r.w, a.w, b.w, F.p, F.np);
+      return r;
+    }
+  }
+#endif
   cios_mul<L>(r.w, a.w, b.w, F.p, F.np);
   return r;
 }

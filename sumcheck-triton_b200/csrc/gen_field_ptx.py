@@ -135,6 +135,92 @@ def gen_mont_mul(L: int) -> str:
     return head + A.render() + "}\n\n"
 
 
+def gen_mont_mul_eo(L: int) -> str:
+    """Montgomery product with separated even/odd accumulators, for p < 2^(32L-1).
+
+    The products a_j b_i of even j land on word pairs (j, j+1) and those of odd j on
+    (j, j+1) with j odd: within each parity no two products share a word, so each parity is
+    ONE carry chain with one multiply-add per word (no second pass for the high halves, as
+    the two-chain CIOS above needs). The accumulator is t = ev + od 2^32: ev holds words
+    0..L-1, od words 1..L. Per outer iteration i:
+
+        ev[0] += ev_old[1]; od = ev_old[2..] + a_odd b_i (the carry of the add flows in);
+        ev = od_old + a_even b_i; od[L-1] += carry      (the shift by one word is a renaming)
+        m = ev[0] nprime; od += p_odd m; ev += p_even m; od[L-1] += carry
+
+    With t < 2p at every iteration start, t + a b_i + m p < 2p (2^32 + 1) < 2^(32(L+1))
+    when p < 2^(32L-1), so no chain carries out of its top word except the two whose carry
+    is added explicitly. Finally t = od + ev[1..] < 2p and one conditional subtraction.
+    Checked bit for bit against big-integer products (tests/test_gpu_parity.py)."""
+    head = (
+        f"template <> __device__ __forceinline__ void ptx_mont_mul_eo<{L}>(uint32_t (&r)[{L}], "
+        f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}], uint32_t np) {{\n"
+    )
+    outs = [(f"r{j}", f"r[{j}]") for j in range(L)]
+    ins = [(f"a{j}", f"a[{j}]") for j in range(L)] + [(f"b{j}", f"b[{j}]") for j in range(L)]
+    ins += [(f"p{j}", f"p[{j}]") for j in range(L)] + [("np", "np")]
+    A = Asm(outs, ins)
+    # PTX registers are virtual: every iteration's ev and od get fresh names (the shift is a
+    # renaming) and the register allocator maps them onto physical registers.
+    A.locals_pred = ["keep"]
+    A.locals_u32 = ["m", "bw"] + [f"d{k}" for k in range(L)] + [f"t{k}" for k in range(L)]
+
+    def bank(tag):
+        names = [f"{tag}{k}" for k in range(L)]
+        A.locals_u32.extend(names)
+        return names
+
+    ev, od = bank("e0_"), bank("o0_")
+    for i in range(L):
+        b = f"b{i}"
+        if i == 0:
+            for j in range(0, L, 2):
+                A.op(f"mul.lo.u32 {ev[j]}, {{}}, {{}};", f"a{j}", b)
+                A.op(f"mul.hi.u32 {ev[j + 1]}, {{}}, {{}};", f"a{j}", b)
+                A.op(f"mul.lo.u32 {od[j]}, {{}}, {{}};", f"a{j + 1}", b)
+                A.op(f"mul.hi.u32 {od[j + 1]}, {{}}, {{}};", f"a{j + 1}", b)
+        else:
+            ne = list(od)  # the new ev is the old od, one word lower
+            no = bank(f"o{i}_")
+            A.op(f"add.cc.u32 {ne[0]}, {ne[0]}, {ev[1]};")
+            src = ev[2:] + ["0", "0"]
+            for j in range(1, L, 2):
+                last = j == L - 1
+                A.op(f"madc.lo.cc.u32 {no[j - 1]}, {{}}, {{}}, {src[j - 1]};", f"a{j}", b)
+                hi = "madc.hi.u32" if last else "madc.hi.cc.u32"
+                A.op(f"{hi} {no[j]}, {{}}, {{}}, {src[j]};", f"a{j}", b)
+            for j in range(0, L, 2):
+                lo = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
+                A.op(f"{lo} {ne[j]}, {{}}, {{}}, {ne[j]};", f"a{j}", b)
+                A.op(f"madc.hi.cc.u32 {ne[j + 1]}, {{}}, {{}}, {ne[j + 1]};", f"a{j}", b)
+            A.op(f"addc.u32 {no[L - 1]}, {no[L - 1]}, 0;")
+            ev, od = ne, no
+        A.op(f"mul.lo.u32 m, {ev[0]}, {{}};", "np")
+        for j in range(1, L, 2):
+            lo = "mad.lo.cc.u32" if j == 1 else "madc.lo.cc.u32"
+            A.op(f"{lo} {od[j - 1]}, m, {{}}, {od[j - 1]};", f"p{j}")
+            A.op(f"madc.hi.cc.u32 {od[j]}, m, {{}}, {od[j]};", f"p{j}")
+        for j in range(0, L, 2):
+            lo = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
+            A.op(f"{lo} {ev[j]}, m, {{}}, {ev[j]};", f"p{j}")
+            A.op(f"madc.hi.cc.u32 {ev[j + 1]}, m, {{}}, {ev[j + 1]};", f"p{j}")
+        A.op(f"addc.u32 {od[L - 1]}, {od[L - 1]}, 0;")
+    # t = od + ev[1..]: words 0..L-1, < 2p
+    t = [f"t{k}" for k in range(L)]
+    A.op(f"add.cc.u32 {t[0]}, {od[0]}, {ev[1]};")
+    for k in range(1, L - 1):
+        A.op(f"addc.cc.u32 {t[k]}, {od[k]}, {ev[k + 1]};")
+    A.op(f"addc.u32 {t[L - 1]}, {od[L - 1]}, 0;")
+    for j in range(L):
+        op = "sub.cc.u32" if j == 0 else "subc.cc.u32"
+        A.op(f"{op} d{j}, {t[j]}, {{}};", f"p{j}")
+    A.op("subc.u32 bw, 0, 0;")
+    A.op("setp.ne.u32 keep, bw, 0;")
+    for j in range(L):
+        A.op(f"selp.b32 {{}}, {t[j]}, d{j}, keep;", f"r{j}")
+    return head + A.render() + "}\n\n"
+
+
 def gen_add(L: int) -> str:
     """r = a + b mod p for a, b < p: add chain, trial subtraction, select."""
     head = (
@@ -195,6 +281,8 @@ def generate() -> str:
         "#pragma once\n#include <cstdint>\n\n",
         "template <int L> __device__ __forceinline__ void ptx_mont_mul(uint32_t (&r)[L], "
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",
+        "template <int L> __device__ __forceinline__ void ptx_mont_mul_eo(uint32_t (&r)[L], "
+        "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",
         "template <int L> __device__ __forceinline__ void ptx_add_mod(uint32_t (&r)[L], "
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L]);\n",
         "template <int L> __device__ __forceinline__ void ptx_sub_mod(uint32_t (&r)[L], "
@@ -203,6 +291,8 @@ def generate() -> str:
     for L in (1, 2, 4, 8):
         parts.append(f"// ---------------- L = {L} ----------------\n")
         parts.append(gen_mont_mul(L))
+        if L >= 4:
+            parts.append(gen_mont_mul_eo(L))
         parts.append(gen_add(L))
         parts.append(gen_sub(L))
     return "".join(parts)

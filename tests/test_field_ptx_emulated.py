@@ -1,0 +1,164 @@
+"""The generated inline-PTX field arithmetic (csrc/field_ptx.cuh), checked on the CPU.
+
+Every carry chain in that header is one asm statement of a small PTX subset. This test parses
+each statement and runs it in a Python emulation of those instructions -- 32-bit registers,
+one carry flag written by the ``.cc`` forms and read by the ``c`` forms, exactly as the PTX ISA
+defines them -- then compares the result with big-integer arithmetic: the Montgomery
+product a b R^-1 mod p, a + b mod p and a - b mod p, on random and edge operands, for the
+reference's four fields and random moduli of each limb count.
+"""
+
+from __future__ import annotations
+
+import random
+import re
+from pathlib import Path
+
+import pytest
+
+HEADER = Path(__file__).resolve().parents[1] / "sumcheck-triton_b200" / "csrc" / "field_ptx.cuh"
+M32 = (1 << 32) - 1
+
+FUNC = re.compile(r"template <> __device__ __forceinline__ void (ptx_\w+)<(\d+)>\((.*?)\) \{\n(.*?)\n\}\n", re.S)
+
+
+def _parse():
+    text = HEADER.read_text()
+    out = {}
+    for name, L, sig, body in FUNC.findall(text):
+        m = re.search(r'asm\((.*?)\n\s*: (.*?)\n\s*: (.*?)\);', body, re.S)
+        asm = "".join(re.findall(r'"((?:[^"\\]|\\.)*)"', m.group(1)))
+        asm = asm.replace("\\n", "\n").replace("\\t", "")
+        outs = re.findall(r'"=&r"\(([^)]*)\)', m.group(2))
+        ins = re.findall(r'"r"\(([^)]*)\)', m.group(3))
+        lines = [ln.strip() for ln in asm.split("\n")]
+        lines = [ln.rstrip(";") for ln in lines if ln and ln not in ("{", "}") and not ln.startswith(".reg")]
+        out[(name, int(L))] = (lines, outs, ins)
+    return out
+
+
+def _run(prog, env_in):
+    """Runs one parsed asm statement; env_in maps C operand expressions (``a[0]``) to values."""
+    lines, outs, ins = prog
+    regs = {}
+    ops = outs + ins
+    for k, e in enumerate(ins):
+        regs[f"%{len(outs) + k}"] = env_in[e] & M32
+    cf = 0
+
+    def val(x):
+        if x in regs:
+            return regs[x]
+        if re.fullmatch(r"-?\d+", x):
+            return int(x) & M32
+        raise KeyError(f"read of unset register {x}")
+
+    for ln in lines:
+        op, rest = ln.split(None, 1)
+        args = [a.strip() for a in rest.split(",")]
+        d = args[0]
+        base = op.split(".")
+        if op.startswith("setp.ne"):
+            regs[d] = int(val(args[1]) != val(args[2]))
+            continue
+        if op.startswith("selp"):
+            regs[d] = val(args[1]) if val(args[3]) else val(args[2])
+            continue
+        if op.startswith("mov"):
+            regs[d] = val(args[1])
+            continue
+        if op.startswith("and"):
+            regs[d] = val(args[1]) & val(args[2])
+            continue
+        cc_out = ".cc" in op
+        kind = base[0]
+        cin = cf if kind in ("madc", "addc", "subc") else 0
+        if kind in ("mul", "mad", "madc"):
+            prod = val(args[1]) * val(args[2])
+            part = (prod & M32) if base[1] == "lo" else (prod >> 32)
+            s = part if kind == "mul" else part + val(args[3]) + cin
+            if cc_out:
+                cf = s >> 32
+            regs[d] = s & M32
+        elif kind in ("add", "addc"):
+            s = val(args[1]) + val(args[2]) + cin
+            if cc_out:
+                cf = s >> 32
+            regs[d] = s & M32
+        elif kind in ("sub", "subc"):
+            s = val(args[1]) - val(args[2]) - cin
+            if cc_out:
+                cf = 1 if s < 0 else 0
+            regs[d] = s & M32
+        else:
+            raise ValueError(f"unknown instruction {ln}")
+    return [regs[f"%{k}"] for k in range(len(outs))]
+
+
+PROGS = _parse()
+FIELDS = {1: [2**32 - 5], 2: [2**64 - 2**32 + 1], 4: [2**127 - 1],
+          8: [0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001]}
+
+
+def _limbs(x, L):
+    return [(x >> (32 * k)) & M32 for k in range(L)]
+
+
+def _val(ws):
+    return sum(w << (32 * k) for k, w in enumerate(ws))
+
+
+def _env(L, p, a, b):
+    env = {f"a[{k}]": w for k, w in enumerate(_limbs(a, L))}
+    env.update({f"b[{k}]": w for k, w in enumerate(_limbs(b, L))})
+    env.update({f"p[{k}]": w for k, w in enumerate(_limbs(p, L))})
+    env["np"] = (-pow(p, -1, 1 << 32)) % (1 << 32)
+    return env
+
+
+def _random_prime(rng, bits):
+    while True:
+        q = rng.randrange(1 << (bits - 1), 1 << bits) | 1
+        if all(pow(w, q - 1, q) == 1 for w in (2, 3, 5, 7)):
+            return q
+
+
+def _moduli(L, eo):
+    rng = random.Random(L * 17 + eo)
+    out = list(FIELDS[L])
+    top = 32 * L - 1 if eo else 32 * L - 2  # even/odd form: p < 2^(32L-1); else the guard's bound
+    out += [_random_prime(rng, top), _random_prime(rng, top - 5)]
+    if eo and L == 8:
+        out.append(2**255 - 19)
+    return out
+
+
+def _operands(p, rng, count):
+    edge = [0, 1, 2, p - 1, p - 2, p // 2, p // 3]
+    for t in range(count):
+        yield (edge[t % len(edge)] if t % 3 == 0 else rng.randrange(p)), rng.randrange(p)
+
+
+@pytest.mark.parametrize("L", [1, 2, 4, 8])
+@pytest.mark.parametrize("name", ["ptx_mont_mul", "ptx_mont_mul_eo"])
+def test_montgomery_product_chains(name, L):
+    if (name, L) not in PROGS:
+        pytest.skip(f"{name}<{L}> is not generated")
+    eo = name.endswith("_eo")
+    for p in _moduli(L, eo):
+        if eo:
+            assert p < 1 << (32 * L - 1)
+        rinv = pow(1 << (32 * L), -1, p)
+        rng = random.Random(p & 0xFFFF)
+        for a, b in _operands(p, rng, 150):
+            got = _val(_run(PROGS[(name, L)], _env(L, p, a, b)))
+            assert got == a * b * rinv % p, (name, L, hex(p), a, b)
+
+
+@pytest.mark.parametrize("L", [1, 2, 4, 8])
+def test_add_and_sub_chains(L):
+    for p in _moduli(L, False):
+        rng = random.Random(p & 0xFFF)
+        for a, b in _operands(p, rng, 100):
+            assert _val(_run(PROGS[("ptx_add_mod", L)], _env(L, p, a, b))) == (a + b) % p
+            assert _val(_run(PROGS[("ptx_sub_mod", L)], _env(L, p, a, b))) == (a - b) % p
