@@ -277,6 +277,52 @@ def profiled_traffic_ratio(L: int):
     return float(m.group(1)) if m else None
 
 
+def busy_ms(intervals) -> float:
+    """Length of the union of [start, end] intervals (ms)."""
+    iv = sorted(intervals)
+    busy, a0, b0 = 0.0, None, None
+    for a, b in iv:
+        if b0 is None or a > b0:
+            if b0 is not None:
+                busy += b0 - a0
+            a0, b0 = a, b
+        else:
+            b0 = max(b0, b)
+    return busy + (b0 - a0 if b0 is not None else 0.0)
+
+
+def group_alone_rooflines(work, batch_items, work_per_round, tuning, device, hbm_peak: float,
+                          imad_rate: float) -> dict:
+    """Each field group of the stream proved alone (its own BatchProver, the same tiles),
+    outside the timed region: its ticks' busy time (CUDA events inside the graph, last of 3
+    timed runs), and its algorithmic bytes and IMAD over that time against the group's own
+    bound -- HBM for the 2-limb group, the IMAD rate for the 8-limb group. In the timed step
+    the two groups share the SMs, so their by-class rates there are not rooflines."""
+    from zkduel_b200.batch import BatchProver
+
+    out = {}
+    for bw in sorted({s.bit_width for s, _f, _e, _t in work.items}):
+        idx = [i for i, (s, _f, _e, _t) in enumerate(work.items) if s.bit_width == bw]
+        bp = BatchProver([batch_items[i] for i in idx], device=device, tuning=tuning)
+        for _ in range(2):
+            bp.run()
+        ms = timed(bp.run, 3, 1, device) / 3
+        cls = bp.tick_times()
+        bp.close()
+        L = cls[0]["limbs"]
+        busy = busy_ms([iv for c in cls for iv in zip(c["start"], c["end"])])
+        b = sum(w[1] for i in idx for w in work_per_round[i])
+        im = sum(w[2] for i in idx for w in work_per_round[i])
+        e = {"proofs": len(idx), "ms_per_step": ms, "busy_ms": busy, "GB/s": b / (busy / 1e3) / 1e9,
+             "TIMAD/s": im / (busy / 1e3) / 1e12}
+        if L >= 4:
+            e.update(bound="imad", frac=e["TIMAD/s"] / (imad_rate / 1e12))
+        else:
+            e.update(bound="hbm", frac=e["GB/s"] / hbm_peak)
+        out[f"L{L}"] = e
+    return out
+
+
 def all_ranks_ok(ok: bool, world: int) -> bool:
     """True on every rank when every rank passes ok (one collective, the same on all ranks)."""
     return max_over_ranks(0.0 if ok else 1.0, world) == 0.0
@@ -581,6 +627,9 @@ def main() -> int:
         roof["by_class"] = {f"L{k}": {"busy_ms": v["ms"], "launches": v["launches"],
                                       "GB/s": v["bytes"] / (v["ms"] / 1e3) / 1e9,
                                       "TIMAD/s": v["imad"] / (v["ms"] / 1e3) / 1e12} for k, v in per_class.items()}
+        if path == "batched":
+            roof["alone"] = group_alone_rooflines(work, batch_items, work_per_round, tuning, device, hbm_peak,
+                                                  imad_rate)
 
     line = {
         "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,

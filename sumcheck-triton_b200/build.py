@@ -16,7 +16,8 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
-LIB = Path(os.environ.get("SC_LIB_OUT", PKG / "zkduel_b200" / "libsumcheck_b200.so"))
+DEFAULT_LIB = PKG / "zkduel_b200" / "libsumcheck_b200.so"
+LIB = Path(os.environ.get("SC_LIB_OUT", DEFAULT_LIB))
 OBJ = Path(os.environ.get("SC_BUILD_DIR", PKG / "_build"))
 CLI = PKG / "bin" / "field_sumcheck_b200"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -43,7 +44,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     sources = [CSRC / s for s in SOURCES]
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "sumcheck_b200.h"]
     if not force and not _stale(LIB, sources + headers):
-        build_cli(os.environ.get("NVCC", "nvcc"))
+        if LIB == DEFAULT_LIB:
+            build_cli(os.environ.get("NVCC", "nvcc"))
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     OBJ.mkdir(exist_ok=True)
@@ -61,7 +63,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         raise subprocess.CalledProcessError(1, f"nvcc {' '.join(failed)}")
     objs = [str(OBJ / (src.stem + ".o")) for src in sources]
     subprocess.check_call([nvcc, *ARCH, "-shared", *objs, "-o", str(LIB)])
-    build_cli(nvcc)
+    if LIB == DEFAULT_LIB:  # the command-line tool links the package's own library only
+        build_cli(nvcc)
     return LIB
 
 
