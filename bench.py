@@ -53,7 +53,7 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 SERVED_COUNT = 20000
 SERVED_LOAD = 0.8
 SERVED_BUDGET = 150 * 10**9
-CAPACITY_MULTIPLES = (1.0, 1.5, 2.0, 3.0, 4.0)  # offered rate / FIFO-plain capacity (1 / E[service])
+CAPACITY_MULTIPLES = (1.0, 1.1, 1.2, 1.3, 1.5, 2.0)  # offered rate / FIFO-plain capacity (1 / E[service])
 CAPACITY_P99_MS = 100.0  # a rate is sustained when throughput >= 95% of it and p99 stays under this
 CPU_SAMPLE_STRIDE = 16
 CPU_SAMPLE_PROOFS = STREAM_COUNT // CPU_SAMPLE_STRIDE  # proofs 0, 16, ..., 496 of the stream

@@ -25,6 +25,7 @@
 #pragma once
 #include <cstdint>
 
+#include "field_gold.cuh"
 #include "field_ptx.cuh"
 
 namespace sc {
@@ -55,17 +56,38 @@ __device__ __forceinline__ Fe<L> fe_zero() {
   return z;
 }
 
+// Goldilocks operations whose carries run on the FMA pipe (field_gold.cuh), by bit:
+// 1 the product, 2 addition, 4 subtraction.
+#ifndef SC_GOLD_FMA
+#define SC_GOLD_FMA 0
+#endif
+
+// The FMA-pipe Goldilocks forms need 1, 0 and 2^32 - 1 as values the compiler cannot fold:
+// the modulus words p = (1, 2^32 - 1) of the kernel parameters.
+template <int L, int K>
+__device__ __forceinline__ GoldK gold_k(const FieldParams<L, K>& F) {
+  return GoldK{F.p[0], F.p[0] >> 1, F.p[L - 1]};
+}
+
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_add(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  ptx_add_mod<L>(r.w, a.w, b.w, F.p);
+  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 2)) {
+    gold_add_fma(r.w, a.w, b.w, gold_k(F));
+  } else {
+    ptx_add_mod<L>(r.w, a.w, b.w, F.p);
+  }
   return r;
 }
 
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_sub(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  ptx_sub_mod<L>(r.w, a.w, b.w, F.p);
+  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 4)) {
+    gold_sub_fma(r.w, a.w, b.w, gold_k(F));
+  } else {
+    ptx_sub_mod<L>(r.w, a.w, b.w, F.p);
+  }
   return r;
 }
 
@@ -146,18 +168,26 @@ __device__ __forceinline__ void gold_mul(uint32_t (&r)[2], const uint32_t (&x32)
 #ifndef SC_MUL_EO
 #define SC_MUL_EO 1
 #endif
+// The Montgomery product of a generic modulus: the even/odd-chain form when it applies
+// (p < 2^(32L - 1), from 4 limbs up), else CIOS with 64-bit intermediates.
 template <int L>
-__device__ __noinline__ Fe<L> cios_mul_call(const Fe<L> a, const Fe<L> b, const FieldParams<L, kFieldGeneric> F) {
-  Fe<L> r;
+__device__ __forceinline__ void mont_mul_generic(uint32_t (&r)[L], const uint32_t (&a)[L], const uint32_t (&b)[L],
+                                                 const FieldParams<L, kFieldGeneric>& F) {
 #if SC_MUL_EO
   if constexpr (L >= 4) {
-    if (F.p[L - 1] < 0x80000000u) {  // p < 2^(32L - 1): the even/odd-chain product applies
-      ptx_mont_mul_eo<L>(r.w, a.w, b.w, F.p, F.np);
-      return r;
+    if (F.p[L - 1] < 0x80000000u) {
+      ptx_mont_mul_eo<L>(r, a, b, F.p, F.np);
+      return;
     }
   }
 #endif
-  cios_mul<L>(r.w, a.w, b.w, F.p, F.np);
+  cios_mul<L>(r, a, b, F.p, F.np);
+}
+
+template <int L>
+__device__ __noinline__ Fe<L> cios_mul_call(const Fe<L> a, const Fe<L> b, const FieldParams<L, kFieldGeneric> F) {
+  Fe<L> r;
+  mont_mul_generic<L>(r.w, a.w, b.w, F);
   return r;
 }
 
@@ -223,7 +253,9 @@ static __device__ __noinline__ Fe<4> m127_mul_call(const Fe<4> a, const Fe<4> b)
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  if constexpr (K == kFieldGoldilocks && L == 2) {
+  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 1)) {
+    gold_mul_fma(r.w, a.w, b.w, gold_k(F));
+  } else if constexpr (K == kFieldGoldilocks && L == 2) {
     gold_mul(r.w, a.w, b.w);
   } else if constexpr (K == kFieldMersenne127 && L == 4) {
     r = m127_mul_call(a, b);
@@ -231,6 +263,8 @@ __device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const Fi
     ptx_mont_mul<1>(r.w, a.w, b.w, F.p, F.np);
   } else if constexpr (L >= SC_OUTLINE_MIN_LIMBS && K == kFieldGeneric) {
     r = cios_mul_call<L>(a, b, F);
+  } else if constexpr (K == kFieldGeneric) {
+    mont_mul_generic<L>(r.w, a.w, b.w, F);
   } else {
     cios_mul<L>(r.w, a.w, b.w, F.p, F.np);
   }

@@ -1,9 +1,11 @@
-"""The generated inline-PTX field arithmetic (csrc/field_ptx.cuh), checked on the CPU.
+"""The inline-PTX field arithmetic (csrc/field_ptx.cuh, generated, and csrc/field_gold.cuh,
+the Goldilocks forms whose carries run on the FMA pipe), checked on the CPU.
 
-Every carry chain in that header is one asm statement of a small PTX subset. This test parses
+Every carry chain in those headers is one asm statement of a small PTX subset. This test parses
 each statement and runs it in a Python emulation of those instructions -- 32-bit registers,
 one carry flag written by the ``.cc`` forms and read by the ``c`` forms, exactly as the PTX ISA
-defines them -- then compares the result with big-integer arithmetic: the Montgomery
+defines them, with a flag written by a subtraction read only by a subtraction and one written by
+an addition or multiply-add read only by those -- then compares the result with big-integer arithmetic: the Montgomery
 product a b R^-1 mod p, a + b mod p and a - b mod p, on random and edge operands, for the
 reference's four fields and random moduli of each limb count.
 """
@@ -16,24 +18,38 @@ from pathlib import Path
 
 import pytest
 
-HEADER = Path(__file__).resolve().parents[1] / "sumcheck-triton_b200" / "csrc" / "field_ptx.cuh"
+CSRC = Path(__file__).resolve().parents[1] / "sumcheck-triton_b200" / "csrc"
+HEADER = CSRC / "field_ptx.cuh"
+GOLD = CSRC / "field_gold.cuh"
 M32 = (1 << 32) - 1
 
 FUNC = re.compile(r"template <> __device__ __forceinline__ void (ptx_\w+)<(\d+)>\((.*?)\) \{\n(.*?)\n\}\n", re.S)
 
 
+def _parse_asm(body):
+    m = re.search(r'asm\((.*?)\n\s*: (.*?)\n\s*: (.*?)\);', body, re.S)
+    asm = "".join(re.findall(r'"((?:[^"\\]|\\.)*)"', m.group(1)))
+    asm = asm.replace("\\n", "\n").replace("\\t", "")
+    outs = re.findall(r'"=&r"\(([^)]*)\)', m.group(2))
+    ins = re.findall(r'"r"\(([^)]*)\)', m.group(3))
+    lines = [ln.strip() for ln in asm.split("\n")]
+    lines = [ln.rstrip(";") for ln in lines if ln and ln not in ("{", "}") and not ln.startswith(".reg")]
+    return lines, outs, ins
+
+
+def _parse_gold():
+    text = GOLD.read_text()
+    out = {}
+    for name, body in re.findall(r"__device__ __forceinline__ void (gold_\w+)\((.*?)\n\}\n", text, re.S):
+        out[name] = _parse_asm(body)
+    return out
+
+
 def _parse():
     text = HEADER.read_text()
     out = {}
-    for name, L, sig, body in FUNC.findall(text):
-        m = re.search(r'asm\((.*?)\n\s*: (.*?)\n\s*: (.*?)\);', body, re.S)
-        asm = "".join(re.findall(r'"((?:[^"\\]|\\.)*)"', m.group(1)))
-        asm = asm.replace("\\n", "\n").replace("\\t", "")
-        outs = re.findall(r'"=&r"\(([^)]*)\)', m.group(2))
-        ins = re.findall(r'"r"\(([^)]*)\)', m.group(3))
-        lines = [ln.strip() for ln in asm.split("\n")]
-        lines = [ln.rstrip(";") for ln in lines if ln and ln not in ("{", "}") and not ln.startswith(".reg")]
-        out[(name, int(L))] = (lines, outs, ins)
+    for name, L, _sig, body in FUNC.findall(text):
+        out[(name, int(L))] = _parse_asm(body)
     return out
 
 
@@ -41,10 +57,10 @@ def _run(prog, env_in):
     """Runs one parsed asm statement; env_in maps C operand expressions (``a[0]``) to values."""
     lines, outs, ins = prog
     regs = {}
-    ops = outs + ins
     for k, e in enumerate(ins):
         regs[f"%{len(outs) + k}"] = env_in[e] & M32
     cf = 0
+    cf_family = None  # which family last wrote the carry flag: "add" (add/mad .cc) or "sub"
 
     def val(x):
         if x in regs:
@@ -73,22 +89,29 @@ def _run(prog, env_in):
         cc_out = ".cc" in op
         kind = base[0]
         cin = cf if kind in ("madc", "addc", "subc") else 0
+        # The flag means a carry after add / mad and a borrow after sub: reading it across
+        # families is not portable (compiled code has given wrong results for it), so a
+        # statement that does is rejected.
+        if kind in ("madc", "addc"):
+            assert cf_family == "add", f"{ln}: reads a carry flag written by a subtraction"
+        if kind == "subc":
+            assert cf_family == "sub", f"{ln}: reads a carry flag written by an addition"
         if kind in ("mul", "mad", "madc"):
             prod = val(args[1]) * val(args[2])
             part = (prod & M32) if base[1] == "lo" else (prod >> 32)
             s = part if kind == "mul" else part + val(args[3]) + cin
             if cc_out:
-                cf = s >> 32
+                cf, cf_family = s >> 32, "add"
             regs[d] = s & M32
         elif kind in ("add", "addc"):
             s = val(args[1]) + val(args[2]) + cin
             if cc_out:
-                cf = s >> 32
+                cf, cf_family = s >> 32, "add"
             regs[d] = s & M32
         elif kind in ("sub", "subc"):
             s = val(args[1]) - val(args[2]) - cin
             if cc_out:
-                cf = 1 if s < 0 else 0
+                cf, cf_family = (1 if s < 0 else 0), "sub"
             regs[d] = s & M32
         else:
             raise ValueError(f"unknown instruction {ln}")
@@ -96,6 +119,7 @@ def _run(prog, env_in):
 
 
 PROGS = _parse()
+GOLD_PROGS = _parse_gold()
 FIELDS = {1: [2**32 - 5], 2: [2**64 - 2**32 + 1], 4: [2**127 - 1],
           8: [0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001]}
 
@@ -162,3 +186,25 @@ def test_add_and_sub_chains(L):
         for a, b in _operands(p, rng, 100):
             assert _val(_run(PROGS[("ptx_add_mod", L)], _env(L, p, a, b))) == (a + b) % p
             assert _val(_run(PROGS[("ptx_sub_mod", L)], _env(L, p, a, b))) == (a - b) % p
+
+
+GOLD_P = 2**64 - 2**32 + 1
+
+
+@pytest.mark.parametrize("name,op", [
+    ("gold_add_fma", lambda a, b: (a + b) % GOLD_P),
+    ("gold_sub_fma", lambda a, b: (a - b) % GOLD_P),
+    ("gold_mul_fma", lambda a, b: a * b * pow(2**64, -1, GOLD_P) % GOLD_P),
+])
+def test_goldilocks_fma_pipe_forms(name, op):
+    assert name in GOLD_PROGS, sorted(GOLD_PROGS)
+    prog = GOLD_PROGS[name]
+    x, y = ("x", "y") if name == "gold_mul_fma" else ("a", "b")
+    rng = random.Random(len(name))
+    edge = [0, 1, 2, GOLD_P - 1, GOLD_P - 2, 2**32, 2**32 - 1, 2**32 + 1, 2**63, GOLD_P // 2]
+    for t in range(4000):
+        a = edge[t % len(edge)] if t % 3 == 0 else rng.randrange(GOLD_P)
+        b = edge[(t // 3) % len(edge)] if t % 5 == 0 else rng.randrange(GOLD_P)
+        env = {f"{x}[0]": a & M32, f"{x}[1]": a >> 32, f"{y}[0]": b & M32, f"{y}[1]": b >> 32,
+               "k.one": 1, "k.zero": 0, "k.eps": M32}
+        assert _val(_run(prog, env)) == op(a, b), (name, a, b)
