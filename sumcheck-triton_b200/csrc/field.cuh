@@ -33,7 +33,9 @@ namespace sc {
 constexpr int kMaxLimbs = 8;
 constexpr int kMaxPoints = 8;  // t = 0..7, degree <= 7
 
-enum FieldKind : int { kFieldGeneric = 0, kFieldGoldilocks = 1, kFieldMersenne127 = 2 };
+// kFieldGoldilocksFma is the Goldilocks field with every carry on the FMA pipe (add and
+// subtract too, field_gold.cuh): the compile-time shape kernels evaluate with it (process_pairs).
+enum FieldKind : int { kFieldGeneric = 0, kFieldGoldilocks = 1, kFieldMersenne127 = 2, kFieldGoldilocksFma = 3 };
 
 template <int L>
 struct Fe {
@@ -57,10 +59,18 @@ __device__ __forceinline__ Fe<L> fe_zero() {
 }
 
 // Goldilocks operations whose carries run on the FMA pipe (field_gold.cuh), by bit:
-// 1 the product, 2 addition, 4 subtraction.
+// 1 the product, 2 addition, 4 subtraction. Measured on B200 (plain_goldilocks, n = 24; the
+// mixed stream's 64-bit group alone): ALU forms 1.94 ms / 6.14 ms; product on the FMA pipe
+// 1.71 / 6.05; product, add and subtract 1.66 / 6.35 (the generic batched evaluator, whose
+// adds are mostly point steps, lost). So the product runs on the FMA pipe everywhere and the
+// compile-time shape kernels, alone, also add and subtract there (kFieldGoldilocksFma).
 #ifndef SC_GOLD_FMA
-#define SC_GOLD_FMA 0
+#define SC_GOLD_FMA 1
 #endif
+#ifndef SC_GOLD_SHAPE_FMA
+#define SC_GOLD_SHAPE_FMA 1
+#endif
+
 
 // The FMA-pipe Goldilocks forms need 1, 0 and 2^32 - 1 as values the compiler cannot fold:
 // the modulus words p = (1, 2^32 - 1) of the kernel parameters.
@@ -72,7 +82,7 @@ __device__ __forceinline__ GoldK gold_k(const FieldParams<L, K>& F) {
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_add(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 2)) {
+  if constexpr (L == 2 && (K == kFieldGoldilocksFma || (K == kFieldGoldilocks && (SC_GOLD_FMA & 2)))) {
     gold_add_fma(r.w, a.w, b.w, gold_k(F));
   } else {
     ptx_add_mod<L>(r.w, a.w, b.w, F.p);
@@ -83,7 +93,7 @@ __device__ __forceinline__ Fe<L> fe_add(const Fe<L>& a, const Fe<L>& b, const Fi
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_sub(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 4)) {
+  if constexpr (L == 2 && (K == kFieldGoldilocksFma || (K == kFieldGoldilocks && (SC_GOLD_FMA & 4)))) {
     gold_sub_fma(r.w, a.w, b.w, gold_k(F));
   } else {
     ptx_sub_mod<L>(r.w, a.w, b.w, F.p);
@@ -253,7 +263,7 @@ static __device__ __noinline__ Fe<4> m127_mul_call(const Fe<4> a, const Fe<4> b)
 template <int L, int K>
 __device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const FieldParams<L, K>& F) {
   Fe<L> r;
-  if constexpr (K == kFieldGoldilocks && L == 2 && (SC_GOLD_FMA & 1)) {
+  if constexpr (L == 2 && (K == kFieldGoldilocksFma || (K == kFieldGoldilocks && (SC_GOLD_FMA & 1)))) {
     gold_mul_fma(r.w, a.w, b.w, gold_k(F));
   } else if constexpr (K == kFieldGoldilocks && L == 2) {
     gold_mul(r.w, a.w, b.w);

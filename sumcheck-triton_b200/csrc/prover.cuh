@@ -296,6 +296,16 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
                                               const Fe<L>& r_prev, const ExprDev& E, uint32_t* sv, uint32_t* sd,
                                               uint64_t first, uint64_t last, uint64_t stride, bool skip1,
                                               Fe<L> (&acc)[DMAX + 1], const FieldParams<L, K>& F) {
+  if constexpr (SHAPE != kShapeGeneric && L == 2 && K == kFieldGoldilocks && SC_GOLD_SHAPE_FMA) {
+    // the shape kernels' folds and points with every Goldilocks carry on the FMA pipe
+    FieldParams<2, kFieldGoldilocksFma> G;
+    G.p[0] = F.p[0];
+    G.p[1] = F.p[1];
+    G.np = F.np;
+    process_pairs<L, kFieldGoldilocksFma, DMAX, SHAPE>(src, dst, src_len, fold, r_prev, E, sv, sd, first, last, stride,
+                                                        skip1, acc, G);
+    return;
+  }
   const int tid = threadIdx.x, nthr = blockDim.x;
   constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
   const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
