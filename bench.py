@@ -88,6 +88,11 @@ def parse():
     ap.add_argument("--profile-batch", action="store_true",
                     help="profile mode: build the mixed stream (--stream-count proofs), run the batch twice, exit")
     ap.add_argument("--stream-count", type=int, default=STREAM_COUNT, help="proofs in the stream (profile mode)")
+    ap.add_argument("--profile-field", type=int, default=0, choices=[0, 64, 256],
+                    help="profile mode: only the proofs of this field width (0: both)")
+    ap.add_argument("--profile-split", action="store_true",
+                    help="profile mode: plain_goldilocks at num_vars 22 proved as 2 emulated ranks (the host "
+                         "gathers the shares), twice, then exit")
     ap.add_argument("--profile-served", action="store_true",
                     help="profile mode: a burst of 120 requests of the served stream (num_vars 12..18) through "
                          "the continuous server, then exit")
@@ -104,12 +109,52 @@ def profile_batch(args) -> int:
     from zkduel_b200.batch import BatchProver
 
     work = Workload(master_seed=0, device=torch.device("cuda", 0), count=args.stream_count)
-    bp = BatchProver([(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items])
+    bp = BatchProver([(e, s.bit_width, s.num_vars, t) for s, _f, e, t in work.items
+                      if args.profile_field in (0, s.bit_width)])
     for _ in range(2):
         bp.run()
     torch.cuda.synchronize()
-    print(json.dumps({"profile_batch": args.stream_count, "table_bytes": work.table_bytes(),
-                      "checksum0": bp.result(0).checksum}))
+    print(json.dumps({"profile_batch": args.stream_count, "field": args.profile_field, "table_bytes": work.table_bytes(),
+                      "checksum0": bp.result(bp.groups[0].indices[0]).checksum}))
+    return 0
+
+
+def profile_split(args) -> int:
+    """One proof split over 2 ranks, emulated in this process on one GPU: each rank's round
+    kernel (ext_out) on its chunk, the host gathers the shares, each rank's commit kernel
+    (split_commit_kernel) finalises the round; twice, the first warms up. plain_goldilocks at
+    num_vars 22: 9 tables x 2^22 x 8 B = 302 MB in two 151 MB chunks (> L2)."""
+    import numpy as np
+    import torch
+
+    from zkduel_b200 import api
+    from zkduel_b200.configs import PLAIN_CONFIGS
+    from zkduel_b200.fields import get_field
+    from zkduel_b200.split import SplitProver
+
+    cfg = PLAIN_CONFIGS["plain_goldilocks"]
+    n, world = 22, 2
+    spec = get_field(cfg.bit_width)
+    enc = api.encode_expression(cfg.expression)
+    kinds = [api._lib.SC_TABLE_BERNOULLI if k == "bernoulli" else api._lib.SC_TABLE_UNIFORM for k in cfg.table_kinds()]
+    t = api.generate_tables(spec, enc.num_vars, n, kinds, cfg.seed)
+    C = (1 << n) // world
+    chunks = [t[:, :, r * C:(r + 1) * C].contiguous() for r in range(world)]
+    for _ in range(2):
+        ranks = [SplitProver(c, cfg.expression, spec, n, world, r) for r, c in enumerate(chunks)]
+        for j in range(ranks[0].local_rounds):
+            shares = np.stack([p.round(j) for p in ranks])
+            for p in ranks:
+                p.commit(j, shares)
+        entries = np.stack([p.last_entries() for p in ranks])
+        for p in ranks:
+            p.finish(entries)
+        out = [p.result() for p in ranks]
+        for p in ranks:
+            p.close()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_split": world, "num_vars": n, "checksum": out[0].checksum,
+                      "ranks_equal": out[0].checksum == out[1].checksum}))
     return 0
 
 
@@ -486,6 +531,8 @@ def main() -> int:
         return profile_aux(args)
     if args.profile_served:
         return profile_served(args)
+    if args.profile_split:
+        return profile_split(args)
     rc = relaunch_ranks(args.gpus)
     if rc is not None:
         return rc
@@ -702,8 +749,8 @@ def profile_aux(args) -> int:
     """Kernels outside the plain configs and the batch, on inputs larger than L2, twice each
     (the first warms up): a generic 256-bit proof at n = 21 (point-parallel kernel, tail
     launch), a generic 64-bit proof at n = 22 (generic round kernel), the refold of a 64-bit
-    n = 22 transcript resumed at round 10 (fold_kernel), and the Montgomery conversion of
-    host tables (convert_tables_kernel)."""
+    n = 22 transcript resumed at round 10 (fold_kernel), the Montgomery conversion of
+    host tables (convert_tables_kernel), and the IMAD-rate probe (imad_probe_kernel)."""
     import torch
 
     from zkduel_b200 import api
@@ -717,11 +764,13 @@ def profile_aux(args) -> int:
     t64 = api.generate_tables(f64, 4, 22, [0] * 4, 2)
     host = api.download_tables(t64, f64)
     half = tr.prove_rounds(t64, e64, f64, 10, tr.start(e64, f64, 22))
+    ctx = api.get_context()
     for _ in range(2):
         api.prove_device(t256, e256, f256, 21, "sha3")
         api.prove_device(t64, e64, f64, 22, "sha3")
         tr.prove_rounds(t64, e64, f64, 22, half)
         api.upload_tables(host, f64)
+        api.calibrate_imad(ctx)  # imad_probe_kernel
     torch.cuda.synchronize()
     print(json.dumps({"profile_aux": True, "bytes_256": t256.numel() * 4, "bytes_64": t64.numel() * 4}))
     return 0
