@@ -86,3 +86,4 @@ __device__ __forceinline__ void gold_mul_fma(uint32_t (&r)[2], const uint32_t (&
 }
 
 }  // namespace sc
+

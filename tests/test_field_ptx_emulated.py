@@ -208,3 +208,4 @@ def test_goldilocks_fma_pipe_forms(name, op):
         env = {f"{x}[0]": a & M32, f"{x}[1]": a >> 32, f"{y}[0]": b & M32, f"{y}[1]": b >> 32,
                "k.one": 1, "k.zero": 0, "k.eps": M32}
         assert _val(_run(prog, env)) == op(a, b), (name, a, b)
+
