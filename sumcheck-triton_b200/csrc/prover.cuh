@@ -617,8 +617,26 @@ __host__ __device__ constexpr int kernel_min_blocks(int L) {
 #define SC_SHAPE_MIN_BLOCKS 2
 #endif
 // Shape kernels of the 1- and 2-limb fields are memory-bound: ask for more resident blocks.
+// The 8-limb shape kernels hold every table's value and difference in registers: at 3 blocks
+// of 128 threads they spilled; at 2 (no spills) plain BLS n = 22 took 3.28 against 3.37 ms
+// with the even/odd product (the batched 8-limb kernels stay at 3, where 2 was 5% slower).
+#ifndef SC_SHAPE_L8_MIN_BLOCKS
+#define SC_SHAPE_L8_MIN_BLOCKS 2
+#endif
+// The batched kernel per limb count and degree class: the 8-limb classes of degree 6-7 hold
+// 7-8 points of 8-limb accumulators and products in registers.
+#ifndef SC_BATCH_L8_HIGH_MIN_BLOCKS
+#define SC_BATCH_L8_HIGH_MIN_BLOCKS SC_L8_MIN_BLOCKS
+#endif
+#ifndef SC_BATCH_L8_HIGH_DMAX
+#define SC_BATCH_L8_HIGH_DMAX 6
+#endif
+__host__ __device__ constexpr int batch_min_blocks(int L, int dmax) {
+  return (L >= 8 && dmax >= SC_BATCH_L8_HIGH_DMAX) ? SC_BATCH_L8_HIGH_MIN_BLOCKS : kernel_min_blocks(L);
+}
 __host__ __device__ constexpr int round_min_blocks(int L, int shape) {
-  return (shape != 0 && L <= 2) ? SC_SHAPE_MIN_BLOCKS : kernel_min_blocks(L);
+  return (shape != 0 && L <= 2) ? SC_SHAPE_MIN_BLOCKS
+                                : ((shape != 0 && L >= 8) ? SC_SHAPE_L8_MIN_BLOCKS : kernel_min_blocks(L));
 }
 
 template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>
@@ -744,7 +762,7 @@ struct BatchTickArgs {
 };
 
 template <int L, int K, int DMAX>
-__global__ void __launch_bounds__(kernel_threads(L), kernel_min_blocks(L))
+__global__ void __launch_bounds__(kernel_threads(L), batch_min_blocks(L, DMAX))
     batch_round_kernel(const BatchTickArgs T, const FieldParams<L, K> F) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ __align__(16) uint32_t g_sm[kMaxPoints * kMaxLimbs];
