@@ -66,16 +66,34 @@ struct sc_split {
 
 namespace {
 
+// The round kernel of a split proof's rounds: the compile-time shape kernel when the host
+// matched one (degree class 4), as for a whole proof; else the generic evaluator.
+template <int L, int K, int D>
+using SplitKern = void (*)(const RoundArgs, const ExprDev, const FieldParams<L, K>);
+
+template <int L, int K, int D>
+SplitKern<L, K, D> split_kernel(const sc_split* S) {
+  if constexpr (D == 4) {
+    if (S->E.shape == kShapeZerocheck) return round_kernel<L, K, 4, kShapeZerocheck>;
+    if (S->E.shape == kShapeAbcg) return round_kernel<L, K, 4, kShapeAbcg>;
+  }
+  return round_kernel<L, K, D>;
+}
+
 template <int L, int K, int D>
 struct SplitSetup {
   static int run(sc_split* S) {
     int threads = kernel_threads(L);
-    const int per_thread = round_smem_words_per_thread(S->K, L) * 4;
-    while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
+    if (S->E.shape != kShapeGeneric && D == 4) {
+      S->smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
+    } else {
+      const int per_thread = round_smem_words_per_thread(S->K, L) * 4;
+      while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
+      S->smem = static_cast<size_t>(threads) * per_thread;
+    }
     S->threads = threads;
-    S->smem = static_cast<size_t>(threads) * per_thread;
     int bps = 0;
-    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, round_kernel<L, K, D>, threads, S->smem));
+    SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, split_kernel<L, K, D>(S), threads, S->smem));
     if (bps < 1) return fail(SC_ERR_UNSUPPORTED, "round kernel does not fit on an SM (K=%d, L=%d)", S->K, L);
     S->grid_max = bps * S->ctx->sm_count;
     return SC_OK;
@@ -90,7 +108,7 @@ struct SplitRound {
     F.np = S->field->hf.np;
     const uint64_t want = (A.pairs + S->threads - 1) / S->threads;
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(std::max<uint64_t>(want, 1), S->grid_max));
-    round_kernel<L, K, D><<<grid, S->threads, S->smem, S->ctx->stream>>>(A, S->E, F);
+    split_kernel<L, K, D>(S)<<<grid, S->threads, S->smem, S->ctx->stream>>>(A, S->E, F);
     SC_CUDA(cudaGetLastError());
     return SC_OK;
   }
