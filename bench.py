@@ -19,15 +19,24 @@ Prints one JSON line (rank 0):
              speed-up);
   roofline   the dominant round kernel (by time) against its bound: integer multiply-adds
              against the measured IMAD rate (256-bit) or bytes against measured HBM GB/s;
-  cpu_baseline  the C oracle (all host threads) on a bounded sample of the same stream;
+  cpu_baseline  the C oracle (all host threads) on a fixed stratified sample of the same
+             stream (32 proofs, about 1/16 of its work; see cpu_sample_specs);
+  plain_configs  the three plain configurations at full size, one proof at a time;
+  reference_cuda  the reference's own CUDA executable (built from its source into
+             oracle/_ref) beside this library's drop-in of it, same arguments, checksums compared;
   served     the served stream (zkduel_b200.streams.served_stream: 20,000 requests over
              2^127 - 1, num_vars log-uniform 12..24, degree 3-7 over up to 8 tables, Poisson
              arrivals at the rate that keeps the FIFO-plain server 80% busy, measured first)
              replayed in real time through the continuous-batching server and through the
              FIFO-plain server, 150 GB admission budget: proofs/s and p50/p90/p99 latency
-             (host-observed completion minus submission) for both.
---impl reference times that CPU port alone on the same workload (the reference's own
-prover is Python-only and cannot run here; the port restates it and is pinned against it).
+             (host-observed completion minus submission) for both; then the capacity sweep
+             (offered rates beyond FIFO's capacity, and a burst) and a burst of requests up to
+             num_vars 26 where the budget binds.
+--impl reference times that CPU port alone on the same fixed sample (the reference's own
+prover is Python-only and its source does not travel here; the port restates it and is
+pinned against it, and reference.py itself was timed at full size where its source is).
+--gpus N runs one rank per GPU: under a launcher the world size must equal N; without one the
+bench re-runs itself under torch.distributed.run with N ranks.
 """
 
 from __future__ import annotations

@@ -33,7 +33,7 @@ extern "C" {
 #define SC_ERR_UNSAFE_MODULUS 2 /* modulus outside the Montgomery product's exactness   */
 #define SC_ERR_CUDA 3           /* a CUDA runtime call failed                            */
 #define SC_ERR_UNSUPPORTED 4    /* outside the compiled limits (degree, tables, terms)  */
-#define SC_ERR_DEVICE 5         /* the device reported an error status                  */
+#define SC_ERR_DEVICE 5         /* the device reported an error status (see sc_prove_resume) */
 #define SC_ERR_NOMEM 6          /* device or host allocation failed                     */
 #define SC_ERR_TIMEOUT 7        /* a bounded wait ran out (sc_server_wait / _drain)     */
 #define SC_ERR_PENDING 8        /* the request has not completed yet                    */
@@ -304,7 +304,11 @@ int sc_tables_tag(int num_tables, const int32_t* table_kinds, uint64_t seed, uin
 /* Proves rounds [rounds done, stop_round) of the transcript's proof on tables_dev (T_0,
  * as for sc_prove) and updates the transcript in place; stop_round = num_rounds completes
  * it. Explicit mode: explicit_challenges holds all num_rounds challenges, and the ones
- * already used must equal the transcript's. Synchronous, like sc_prove. */
+ * already used must equal the transcript's. Where the first resumed round would take g(1)
+ * from the recorded claim (a round of 2^12 pairs or more), it evaluates g(1) from the
+ * tables and checks g(0) + g(1) against that claim on the device: tables other than the
+ * ones the recorded rounds were proved on, or an altered claim, fail with SC_ERR_DEVICE
+ * (device status 1) and leave the transcript unchanged. Synchronous, like sc_prove. */
 int sc_prove_resume(sc_ctx* ctx, const sc_field* field, const sc_expr* expr,
                     const uint32_t* tables_dev, const uint32_t* explicit_challenges, int stop_round,
                     uint32_t* transcript, uint64_t words);

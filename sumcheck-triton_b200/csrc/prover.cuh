@@ -583,8 +583,9 @@ __host__ __device__ constexpr int round_smem_words_per_thread(int K, int L) { re
 
 // Launch shape per limb count: 8-limb kernels hold (DMAX + 1) x 8-word point arrays per
 // thread, so they run 128-thread blocks and ask the compiler for at least 3 blocks per SM
-// (<= 168 registers; on B200 the mixed 512-proof stream ran 10% slower with 2 or 4);
-// smaller fields run 256-thread blocks.
+// (<= 168 registers; on B200 the mixed 512-proof stream ran 10% slower with 2 or 4 blocks
+// with the C++ product, 5% and 4% slower with the even/odd product); smaller fields run
+// 256-thread blocks.
 __host__ __device__ constexpr int kernel_threads(int L) { return L >= 8 ? 128 : 256; }
 #ifndef SC_PP_MIN_LIMBS
 #define SC_PP_MIN_LIMBS 8
