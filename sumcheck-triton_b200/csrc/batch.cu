@@ -34,9 +34,14 @@ constexpr bool kBatchTails = SC_BATCH_TAILS != 0;
 #endif
 constexpr bool kBatchDmax6 = SC_BATCH_DMAX6 != 0;  // see dispatch_dmax
 
+// Tails for fields of at most this many limbs only (0: none).
+#ifndef SC_BATCH_TAIL_MAX_L
+#define SC_BATCH_TAIL_MAX_L 0
+#endif
+
 // Ticks proof p takes: one per round, or up to its first one-tile round with tails.
-inline int proof_ticks(int n, uint64_t tile) {
-  if constexpr (kBatchTails) {
+inline int proof_ticks(int n, uint64_t tile, int L) {
+  if (kBatchTails || L <= SC_BATCH_TAIL_MAX_L) {
     for (int t = 0; t < n; ++t)
       if ((uint64_t{1} << n) >> (t + 1) <= tile) return t + 1;
   }
@@ -202,7 +207,7 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
       return rc;
     C.max_rounds = 0;  // ticks of the class
     for (int p : C.proofs)
-      C.max_rounds = std::max(C.max_rounds, proof_ticks(B->n[p], static_cast<uint64_t>(C.threads) * B->ppt[p]));
+      C.max_rounds = std::max(C.max_rounds, proof_ticks(B->n[p], static_cast<uint64_t>(C.threads) * B->ppt[p], B->L));
     B->classes.push_back(std::move(C));
   }
   // per-proof state and fold buffers (16-byte aligned carve-outs of two pools)
@@ -239,7 +244,7 @@ int batch_setup(sc_batch* B, const sc_expr* const* exprs, const uint32_t* const*
       int tick_items = 0;
       for (int p : C.proofs) {
         const uint64_t tile = static_cast<uint64_t>(C.threads) * B->ppt[p];
-        const int ticks = proof_ticks(B->n[p], tile);
+        const int ticks = proof_ticks(B->n[p], tile, B->L);
         if (t >= ticks) continue;
         const int n = B->n[p];
         const uint64_t N = uint64_t{1} << n;
