@@ -4,8 +4,9 @@ Run from the repository root (the build runs it when the header is missing or ol
 
     python sumcheck-triton_b200/csrc/gen_field_ptx.py
 
-Each operation (Montgomery product, modular add, modular subtract) for a limb count L in
-{1, 2, 4, 8} is ONE asm statement, generated here as straight-line PTX:
+Each operation -- the two-chain Montgomery product (L = 1), the even/odd-chain product
+(L = 4, 8; for p < 2^(32 L - 1)), modular add and subtract (L = 1, 2, 4, 8) -- is ONE asm
+statement, generated here as straight-line PTX:
 
 * the carry flag is only meaningful inside one statement (the compiler may place its own
   ``.cc`` instructions between statements), so every chain must be inside one;
@@ -290,7 +291,10 @@ def generate() -> str:
     ]
     for L in (1, 2, 4, 8):
         parts.append(f"// ---------------- L = {L} ----------------\n")
-        parts.append(gen_mont_mul(L))
+        # The two-chain product is the kernels' choice at one limb only; from two limbs up the
+        # special reductions, the C++ CIOS or the even/odd form measured faster (field.cuh).
+        if L == 1:
+            parts.append(gen_mont_mul(L))
         if L >= 4:
             parts.append(gen_mont_mul_eo(L))
         parts.append(gen_add(L))
