@@ -203,12 +203,6 @@ template <int L, int K, int D>
 struct SetRoundAttrs {
   static int run() {
     SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-    if constexpr (D == 4 && shape_in_smem(L, kShapeAbcg)) {  // shape kernels staging values in shared memory
-      SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, 4, kShapeAbcg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kMaxDynSmem));
-      SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, 4, kShapeZerocheck>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-    }
     return SC_OK;
   }
 };
