@@ -110,9 +110,6 @@ struct ProveRun {
       const int per_thread = round_smem_words_per_thread(K_, L) * 4;
       while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
       smem = static_cast<size_t>(threads) * per_thread;
-    } else if (shape_in_smem(L, shape)) {  // every role's value and difference, per thread
-      smem = std::max<size_t>(static_cast<size_t>(threads) * 2 * shape_tables(shape) * L * 4,
-                              static_cast<size_t>(threads / 32) * kMaxPoints * L * 4);
     } else {
       smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
     }

@@ -276,35 +276,6 @@ __device__ __forceinline__ Fe<L> shape_value(const Fe<L> (&v)[6], const FieldPar
   return fe_mul(v[3], s, F);
 }
 
-// The shapes' values at one point read from this thread's shared-memory slots (role order):
-// the 8-limb shape kernels keep a pair's values and differences there (process_pairs).
-template <int L, int K>
-__device__ __forceinline__ Fe<L> shape_value_sm(const uint32_t* sv, int tid, int nthr, const FieldParams<L, K>& F,
-                                                std::integral_constant<int, kShapeZerocheck>) {
-  auto v = [&](int i) { return sm_get<L>(sv, i, tid, nthr); };
-  const Fe<L> u = fe_add(v(0), fe_mul(v(5), v(4), F), F);  // S1 + M X2
-  Fe<L> s = fe_mul(v(1), u, F);                            // X1 (S1 + M X2)
-  s = fe_add(s, fe_mul(v(3), v(4), F), F);                 // + S2 X2
-  s = fe_sub(s, fe_mul(v(6), v(7), F), F);                 // - S4 X3
-  s = fe_add(s, v(8), F);                                  // + S5
-  return fe_mul(v(2), s, F);                               // F (...)
-}
-
-template <int L, int K>
-__device__ __forceinline__ Fe<L> shape_value_sm(const uint32_t* sv, int tid, int nthr, const FieldParams<L, K>& F,
-                                                std::integral_constant<int, kShapeAbcg>) {
-  auto v = [&](int i) { return sm_get<L>(sv, i, tid, nthr); };
-  const Fe<L> s = fe_add(fe_mul(fe_mul(v(0), v(1), F), v(2), F), fe_mul(v(4), v(5), F), F);
-  return fe_mul(v(3), s, F);
-}
-
-// 8-limb shape kernels: a pair's values and differences in shared memory (slots as the
-// generic evaluator's) instead of registers, so the kernel fits more warps per SM.
-#ifndef SC_SHAPE_L8_SMEM
-#define SC_SHAPE_L8_SMEM 0
-#endif
-__host__ __device__ constexpr bool shape_in_smem(int L, int shape) { return SC_SHAPE_L8_SMEM && shape != 0 && L >= 8; }
-
 // Folds (if fold) and evaluates pairs q = first, first + stride, ... < last, adding the
 // point sums into acc. Generic: every table's value and difference go to this block's
 // [K][L][nthr] shared arrays sv / sd for eval_pair. Shape kernels keep them in registers
@@ -338,49 +309,6 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
   const int tid = threadIdx.x, nthr = blockDim.x;
   constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
   const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
-  if constexpr (shape_in_smem(L, SHAPE)) {
-    for (uint64_t q = first; q < last; q += stride) {
-#pragma unroll 1
-      for (int i = 0; i < NR; ++i) {
-        const int k = E.role[i];
-        Fe<L> e, o;
-        if (fold) {
-          Fe<L> x0, x1, x2, x3;
-#pragma unroll
-          for (int l = 0; l < L; ++l) {
-            const uint4 v = __ldcs(reinterpret_cast<const uint4*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
-            x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
-          }
-          e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
-          o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
-          const uint64_t dst_len = src_len >> 1;
-#pragma unroll
-          for (int l = 0; l < L; ++l)
-            reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(k) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
-        } else {
-#pragma unroll
-          for (int l = 0; l < L; ++l) {
-            const uint2 v = __ldcs(reinterpret_cast<const uint2*>(src + (static_cast<uint64_t>(k) * L + l) * src_len) + q);
-            e.w[l] = v.x; o.w[l] = v.y;
-          }
-        }
-        sm_put<L>(sv, i, tid, nthr, e);
-        sm_put<L>(sd, i, tid, nthr, fe_sub(o, e, F));
-      }
-      constexpr int D = 4;
-      static_assert(DMAX >= D, "shape kernels evaluate degree-4 shapes");
-      acc[0] = fe_add(acc[0], shape_value_sm<L, K>(sv, tid, nthr, F, std::integral_constant<int, SHAPE>{}), F);
-#pragma unroll
-      for (int t = 1; t <= D; ++t) {
-#pragma unroll 1
-        for (int i = 0; i < NR; ++i)
-          sm_put<L>(sv, i, tid, nthr, fe_add(sm_get<L>(sv, i, tid, nthr), sm_get<L>(sd, i, tid, nthr), F));
-        if (t == 1 && skip1) continue;
-        acc[t] = fe_add(acc[t], shape_value_sm<L, K>(sv, tid, nthr, F, std::integral_constant<int, SHAPE>{}), F);
-      }
-    }
-    return;
-  }
 #pragma unroll(SHAPE == kShapeGeneric ? 1 : kPairUnroll)
   for (uint64_t q = first; q < last; q += stride) {
     Fe<L> sh_v[NR], sh_d[NR];
@@ -707,14 +635,9 @@ __host__ __device__ constexpr int kernel_min_blocks(int L) {
 __host__ __device__ constexpr int batch_min_blocks(int L, int dmax) {
   return (L >= 8 && dmax >= SC_BATCH_L8_HIGH_DMAX) ? SC_BATCH_L8_HIGH_MIN_BLOCKS : kernel_min_blocks(L);
 }
-#ifndef SC_SHAPE_L8_SMEM_MIN_BLOCKS
-#define SC_SHAPE_L8_SMEM_MIN_BLOCKS 4
-#endif
 __host__ __device__ constexpr int round_min_blocks(int L, int shape) {
-  return (shape != 0 && L <= 2)
-             ? SC_SHAPE_MIN_BLOCKS
-             : ((shape != 0 && L >= 8) ? (shape_in_smem(L, shape) ? SC_SHAPE_L8_SMEM_MIN_BLOCKS : SC_SHAPE_L8_MIN_BLOCKS)
-                                       : kernel_min_blocks(L));
+  return (shape != 0 && L <= 2) ? SC_SHAPE_MIN_BLOCKS
+                                : ((shape != 0 && L >= 8) ? SC_SHAPE_L8_MIN_BLOCKS : kernel_min_blocks(L));
 }
 
 template <int L, int K, int DMAX, int SHAPE = kShapeGeneric>

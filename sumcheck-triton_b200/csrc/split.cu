@@ -86,8 +86,6 @@ struct SplitSetup {
     int threads = kernel_threads(L);
     if (S->E.shape != kShapeGeneric && D == 4) {
       S->smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
-      if (shape_in_smem(L, S->E.shape))  // every role's value and difference, per thread
-        S->smem = std::max<size_t>(S->smem, static_cast<size_t>(threads) * 2 * shape_tables(S->E.shape) * L * 4);
     } else {
       const int per_thread = round_smem_words_per_thread(S->K, L) * 4;
       while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
