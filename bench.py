@@ -720,7 +720,8 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         line["reference_cuda"] = reference_cuda_compare()
     if rank == 0 and world == 1 and not args.no_plain_configs:
-        line["plain_configs"] = plain_configs_measure(device, cpu=not args.no_cpu)
+        line["plain_configs"] = plain_configs_measure(device, cpu=not args.no_cpu, hbm_peak=hbm_peak,
+                                                      imad_rate=imad_rate)
     if args.served > 0:
         del batcher, steps_fn, work
         torch.cuda.empty_cache()
@@ -785,7 +786,8 @@ def profile_aux(args) -> int:
     return 0
 
 
-def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20) -> dict:
+def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20, hbm_peak: float | None = None,
+                          imad_rate: float | None = None) -> dict:
     """The three plain configs one proof at a time at full size, tables resident: per-proof
     device time (CUDA events) as p50 / p99 and proofs/s. Beside it the C port of the
     reference's CPU prover (every host thread) on the same tables: at full size for the
@@ -795,7 +797,7 @@ def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20) -> dict:
 
     from oracle import c_oracle as C
     from oracle import oracle as O
-    from zkduel_b200 import api
+    from zkduel_b200 import api, roofline
     from zkduel_b200.configs import PLAIN_CONFIGS
     from zkduel_b200.fields import get_field
 
@@ -824,6 +826,19 @@ def plain_configs_measure(device, cpu: bool = True, cpu_vars: int = 20) -> dict:
         entry = {"num_vars": n, "gpu": {"p50_ms": ms[len(ms) // 2], "p99_ms": ms[min(len(ms) - 1, int(0.99 * len(ms)))],
                                         "proofs_per_s": 1e3 * len(ms) / sum(ms), "proofs": len(ms),
                                         "timer": "CUDA events around each prove_device (results on the host)"}}
+        # the whole proof against its bound (canonical counts, zkduel_b200.roofline): HBM for
+        # the 64-bit zerocheck, the IMAD rate for 256 bits; the 32-bit config is L2-resident
+        p50_s = entry["gpu"]["p50_ms"] / 1e3
+        if spec.limbs == 2 and hbm_peak:
+            b = roofline.proof_bytes(enc.num_vars, spec.limbs, n)
+            entry["roofline"] = {"bound": "hbm", "algorithmic_bytes": b, "achieved": b / p50_s / 1e9,
+                                 "peak": hbm_peak, "unit": "GB/s", "frac": b / p50_s / 1e9 / hbm_peak}
+        elif spec.limbs == 8 and imad_rate:
+            im = roofline.proof_imad(enc.num_vars, spec.limbs, enc.degree, sum(t - 1 for t in enc.term_lens), n)
+            entry["roofline"] = {"bound": "imad", "algorithmic_imad": im, "achieved": im / p50_s / 1e12,
+                                 "peak": imad_rate / 1e12, "unit": "TIMAD/s", "frac": im / p50_s / imad_rate}
+        else:
+            entry["roofline"] = {"bound": "latency", "note": "tables resident in L2 (2 x 256 KiB): p50 / p99 latency"}
         if cpu:
             nc = n if n <= 16 else cpu_vars
             terms, k = O.indexed_terms(cfg.expression)
