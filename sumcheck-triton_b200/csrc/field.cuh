@@ -281,6 +281,54 @@ __device__ __forceinline__ Fe<L> fe_mul(const Fe<L>& a, const Fe<L>& b, const Fi
   return r;
 }
 
+// Lazy Goldilocks arithmetic (field_gold.cuh): values are any representative in [0, 2^64)
+// between operations and are made canonical (gold_canon) only where they leave a thread.
+// Which forms, measured on B200 (plain_goldilocks n = 24 p50 / the mixed stream's 64-bit
+// group alone, 240 proofs; canonical arithmetic 1.65 / 6.07 ms):
+//   point steps (value + canonical difference) on the ALU, SC_GOLD_LAZY_STEP_ALU = 1:
+//     1.60 / 5.93 ms; the same on the FMA pipe (five multiply-adds): 1.64 / 6.10 ms;
+//   the product gold_mul_fma (exact on any operands), SC_GOLD_MUL_ANY = 0; gold_mul_any, with
+//     four more of its steps on the FMA pipe, took the shape kernel to 1.72 ms.
+__device__ __forceinline__ Fe<2> gl_add(const Fe<2>& a, const Fe<2>& b, const GoldK k) {
+  Fe<2> r;
+  gold_add_lazy(r.w, a.w, b.w, k);
+  return r;
+}
+#ifndef SC_GOLD_LAZY_STEP_ALU
+#define SC_GOLD_LAZY_STEP_ALU 1
+#endif
+#ifndef SC_GOLD_MUL_ANY
+#define SC_GOLD_MUL_ANY 0
+#endif
+__device__ __forceinline__ Fe<2> gl_add_c(const Fe<2>& a, const Fe<2>& b_canonical, const GoldK k) {
+  Fe<2> r;
+#if SC_GOLD_LAZY_STEP_ALU
+  gold_add_lazy_c_alu(r.w, a.w, b_canonical.w, k);
+#else
+  gold_add_lazy_c(r.w, a.w, b_canonical.w, k);
+#endif
+  return r;
+}
+__device__ __forceinline__ Fe<2> gl_sub(const Fe<2>& a, const Fe<2>& b, const GoldK k) {
+  Fe<2> r;
+  gold_sub_lazy(r.w, a.w, b.w, k);
+  return r;
+}
+__device__ __forceinline__ Fe<2> gl_mul(const Fe<2>& a, const Fe<2>& b, const GoldK k) {
+  Fe<2> r;
+#if SC_GOLD_MUL_ANY
+  gold_mul_any(r.w, a.w, b.w, k);
+#else
+  gold_mul_fma(r.w, a.w, b.w, k);  // also exact on operands in [0, 2^64) (see gold_mul_any)
+#endif
+  return r;
+}
+__device__ __forceinline__ Fe<2> gl_canon(const Fe<2>& a, const GoldK k) {
+  Fe<2> r;
+  gold_canon(r.w, a.w, k);
+  return r;
+}
+
 template <int L>
 __device__ __forceinline__ bool fe_is_zero(const Fe<L>& a) {
   uint32_t o = 0;

@@ -209,3 +209,51 @@ def test_goldilocks_fma_pipe_forms(name, op):
                "k.one": 1, "k.zero": 0, "k.eps": M32}
         assert _val(_run(prog, env)) == op(a, b), (name, a, b)
 
+
+RINV64 = pow(2**64, -1, GOLD_P)
+# the lazy forms: (name, operand names, second operand canonical?, residue of the result)
+LAZY = [
+    ("gold_add_lazy_c", ("a", "b"), True, lambda a, b: (a + b) % GOLD_P),
+    ("gold_add_lazy_c_alu", ("a", "b"), True, lambda a, b: (a + b) % GOLD_P),
+    ("gold_add_lazy", ("a", "b"), False, lambda a, b: (a + b) % GOLD_P),
+    ("gold_sub_lazy", ("a", "b"), False, lambda a, b: (a - b) % GOLD_P),
+    ("gold_mul_any", ("x", "y"), False, lambda a, b: a * b * RINV64 % GOLD_P),
+    ("gold_mul_fma", ("x", "y"), False, lambda a, b: a * b * RINV64 % GOLD_P),
+]
+
+
+@pytest.mark.parametrize("name,names,b_canonical,op", LAZY)
+def test_goldilocks_lazy_forms(name, names, b_canonical, op):
+    """Operands anywhere in [0, 2^64) -- the non-canonical band [p, 2^64) included -- give a
+    representative of the right residue (gold_mul_fma too: the lazy kernels use it on any
+    operands); gold_mul_any on operands below p equals gold_mul_fma."""
+    assert name in GOLD_PROGS, sorted(GOLD_PROGS)
+    prog = GOLD_PROGS[name]
+    x, y = names
+    rng = random.Random(len(name) * 7)
+    top = 2**64
+    edge = [0, 1, 2, GOLD_P - 1, GOLD_P, GOLD_P + 1, top - 1, top - 2, top - 2**32, 2**32 - 1, 2**32,
+            2**63, GOLD_P - 2**32]
+    for t in range(6000):
+        a = edge[t % len(edge)] if t % 3 == 0 else rng.randrange(top if t % 2 else GOLD_P)
+        bmax = GOLD_P if b_canonical else top
+        b = edge[(t // 3) % len(edge)] if t % 5 == 0 else rng.randrange(bmax if t % 4 else GOLD_P)
+        if b_canonical:
+            b %= GOLD_P
+        env = {f"{x}[0]": a & M32, f"{x}[1]": a >> 32, f"{y}[0]": b & M32, f"{y}[1]": b >> 32,
+               "k.one": 1, "k.zero": 0, "k.eps": M32}
+        got = _val(_run(prog, env))
+        assert got % GOLD_P == op(a, b), (name, a, b)
+        if name == "gold_mul_any" and a < GOLD_P and b < GOLD_P:
+            assert got == _val(_run(GOLD_PROGS["gold_mul_fma"], env)) < GOLD_P
+
+
+def test_goldilocks_canon():
+    prog = GOLD_PROGS["gold_canon"]
+    rng = random.Random(5)
+    vals = [0, 1, GOLD_P - 1, GOLD_P, GOLD_P + 1, 2**64 - 1, 2**64 - 2**32, 2**64 - 2**32 + 2]
+    vals += [rng.randrange(2**64) for _ in range(3000)]
+    for a in vals:
+        env = {"a[0]": a & M32, "a[1]": a >> 32, "k.one": 1, "k.zero": 0, "k.eps": M32}
+        assert _val(_run(prog, env)) == a % GOLD_P, a
+
