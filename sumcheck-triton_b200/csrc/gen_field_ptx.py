@@ -5,7 +5,8 @@ Run from the repository root (the build runs it when the header is missing or ol
     python sumcheck-triton_b200/csrc/gen_field_ptx.py
 
 Each operation -- the two-chain Montgomery product (L = 1), the even/odd-chain product
-(L = 4, 8; for p < 2^(32 L - 1)), modular add and subtract (L = 1, 2, 4, 8) -- is ONE asm
+(L = 4, 8; for p < 2^(32 L - 1); also in a form for moduli with p_0 = 1, p_1 = 2^32 - 1),
+modular add and subtract (L = 1, 2, 4, 8) -- is ONE asm
 statement, generated here as straight-line PTX:
 
 * the carry flag is only meaningful inside one statement (the compiler may place its own
@@ -136,7 +137,7 @@ def gen_mont_mul(L: int) -> str:
     return head + A.render() + "}\n\n"
 
 
-def gen_mont_mul_eo(L: int) -> str:
+def gen_mont_mul_eo(L: int, low_one: bool = False) -> str:
     """Montgomery product with separated even/odd accumulators, for p < 2^(32L-1).
 
     The products a_j b_i of even j land on word pairs (j, j+1) and those of odd j on
@@ -152,9 +153,17 @@ def gen_mont_mul_eo(L: int) -> str:
     With t < 2p at every iteration start, t + a b_i + m p < 2p (2^32 + 1) < 2^(32(L+1))
     when p < 2^(32L-1), so no chain carries out of its top word except the two whose carry
     is added explicitly. Finally t = od + ev[1..] < 2p and one conditional subtraction.
-    Checked bit for bit against big-integer products (tests/test_gpu_parity.py)."""
+    Checked bit for bit against big-integer products (tests/test_gpu_parity.py).
+
+    low_one: the form for moduli whose two low words are p_0 = 1 and p_1 = 2^32 - 1 (the
+    BLS12-381 scalar field): nprime = -1, so m = -ev[0], and the three multiplies of a row
+    that involve p_0, p_1 and nprime become ALU operations. m p_0 = m is an addition; m p_1 =
+    m 2^32 - m has low word -m mod 2^32 = ev[0] and high word m - (m != 0), with m != 0
+    exactly when ev[0] != 0. Every row then issues 3 fewer multiply instructions (of 17 for
+    L = 8), and the multiplies are what bound the product (the FMA-heavy pipe)."""
+    name = "ptx_mont_mul_eo1" if low_one else "ptx_mont_mul_eo"
     head = (
-        f"template <> __device__ __forceinline__ void ptx_mont_mul_eo<{L}>(uint32_t (&r)[{L}], "
+        f"template <> __device__ __forceinline__ void {name}<{L}>(uint32_t (&r)[{L}], "
         f"const uint32_t (&a)[{L}], const uint32_t (&b)[{L}], const uint32_t (&p)[{L}], uint32_t np) {{\n"
     )
     outs = [(f"r{j}", f"r[{j}]") for j in range(L)]
@@ -165,6 +174,8 @@ def gen_mont_mul_eo(L: int) -> str:
     # renaming) and the register allocator maps them onto physical registers.
     A.locals_pred = ["keep"]
     A.locals_u32 = ["m", "bw"] + [f"d{k}" for k in range(L)] + [f"t{k}" for k in range(L)]
+    if low_one:
+        A.locals_u32 += ["nz", "h1"]
 
     def bank(tag):
         names = [f"{tag}{k}" for k in range(L)]
@@ -196,12 +207,23 @@ def gen_mont_mul_eo(L: int) -> str:
                 A.op(f"madc.hi.cc.u32 {ne[j + 1]}, {{}}, {{}}, {ne[j + 1]};", f"a{j}", b)
             A.op(f"addc.u32 {no[L - 1]}, {no[L - 1]}, 0;")
             ev, od = ne, no
-        A.op(f"mul.lo.u32 m, {ev[0]}, {{}};", "np")
-        for j in range(1, L, 2):
+        if low_one:
+            # m = -ev[0]; m p_1 = (ev[0], m - (ev[0] != 0)); m p_0 = (m, 0)
+            A.op(f"sub.u32 m, 0, {ev[0]};")
+            A.op(f"min.u32 nz, {ev[0]}, 1;")
+            A.op("sub.u32 h1, m, nz;")
+            A.op(f"add.cc.u32 {od[0]}, {od[0]}, {ev[0]};")
+            A.op(f"addc.cc.u32 {od[1]}, {od[1]}, h1;")
+        else:
+            A.op(f"mul.lo.u32 m, {ev[0]}, {{}};", "np")
+        for j in range(3 if low_one else 1, L, 2):
             lo = "mad.lo.cc.u32" if j == 1 else "madc.lo.cc.u32"
             A.op(f"{lo} {od[j - 1]}, m, {{}}, {od[j - 1]};", f"p{j}")
             A.op(f"madc.hi.cc.u32 {od[j]}, m, {{}}, {od[j]};", f"p{j}")
-        for j in range(0, L, 2):
+        if low_one:
+            A.op(f"add.cc.u32 {ev[0]}, {ev[0]}, m;")
+            A.op(f"addc.cc.u32 {ev[1]}, {ev[1]}, 0;")
+        for j in range(2 if low_one else 0, L, 2):
             lo = "mad.lo.cc.u32" if j == 0 else "madc.lo.cc.u32"
             A.op(f"{lo} {ev[j]}, m, {{}}, {ev[j]};", f"p{j}")
             A.op(f"madc.hi.cc.u32 {ev[j + 1]}, m, {{}}, {ev[j + 1]};", f"p{j}")
@@ -284,6 +306,8 @@ def generate() -> str:
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",
         "template <int L> __device__ __forceinline__ void ptx_mont_mul_eo(uint32_t (&r)[L], "
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",
+        "template <int L> __device__ __forceinline__ void ptx_mont_mul_eo1(uint32_t (&r)[L], "
+        "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L], uint32_t np);\n",
         "template <int L> __device__ __forceinline__ void ptx_add_mod(uint32_t (&r)[L], "
         "const uint32_t (&a)[L], const uint32_t (&b)[L], const uint32_t (&p)[L]);\n",
         "template <int L> __device__ __forceinline__ void ptx_sub_mod(uint32_t (&r)[L], "
@@ -297,6 +321,7 @@ def generate() -> str:
             parts.append(gen_mont_mul(L))
         if L >= 4:
             parts.append(gen_mont_mul_eo(L))
+            parts.append(gen_mont_mul_eo(L, low_one=True))
         parts.append(gen_add(L))
         parts.append(gen_sub(L))
     return "".join(parts)
