@@ -15,6 +15,16 @@ default). For each configuration:
 4. its ``(claim0, round evaluations)`` are compared with the C oracle's, decoded from
    Montgomery form -- a full-size pin of the C oracle against the reference itself.
 
+Two stream samples (``stream_batched``, ``stream_served``) time the same function on a
+seeded, stratified sample of the batched and the served proof streams: every proof of the
+sample runs in a ``multiprocessing`` pool (spawn) with one worker per host core; each worker
+times ``sumcheck_reference`` around the call alone, on its one thread. Reported: the sum of
+those per-proof times (the sample proved on one thread), the pool's wall time (the sample
+proved on every core), proofs/s for both, and whether every proof equals the C oracle's.
+The batched sample is the bench's CPU sample (32 proofs, every 16th of the 512-proof stream
+sorted by field and size, about 1/16 of its work); the served sample is every 1000th of the
+20,000-request stream (seed 1) sorted by size, from the 500th on.
+
 Writes ``oracle/reference_py_timings.json`` (host, CPU model, nproc, seconds, match).
 
     SUMCHECK_REFERENCE=<reference checkout> python oracle/time_reference_py.py [config ...]
@@ -102,6 +112,79 @@ def run(name: str, ref_src: Path) -> dict:
             "outputs_equal_c_oracle": bool(match)}
 
 
+STREAMS = ("stream_batched", "stream_served")
+
+
+def stream_sample(name: str):
+    """(spec, bit width) of every proof in the named stream sample."""
+    from zkduel_b200.streams import served_stream
+
+    if name == "stream_batched":
+        import bench  # the bench's own fixed CPU sample
+
+        return [(sp, sp.bit_width) for sp in bench.cpu_sample_specs()]
+    reqs = sorted(served_stream(20000, rate_per_s=1.0, seed=1), key=lambda r: (r.spec.num_vars, r.spec.index))
+    return [(r.spec, 128) for r in reqs[500::1000]]
+
+
+def _stream_worker(job):
+    """One proof of a stream sample in a pool worker: C-oracle tables and SHA3 challenges,
+    then the reference's ``sumcheck_reference`` timed alone; returns (index, seconds, equal)."""
+    ref_src, spec, bw = job
+    if ref_src not in sys.path:
+        sys.path.insert(0, ref_src)
+    from zkduel.reference import sumcheck_reference  # the reference's own code
+
+    from oracle import c_oracle
+    from oracle.oracle import indexed_terms
+    from zkduel_b200.fields import get_field
+
+    f = get_field(bw)
+    p, L, n = f.modulus, f.limbs, spec.num_vars
+    names = spec.var_names
+    terms, k = indexed_terms(spec.expression, names)
+    tables = c_oracle.generate(p, L, [0] * k, n, spec.seed)
+    want = c_oracle.prove(terms, k, p, L, tables, "sha3", threads=1)
+    chals = [from_mont(want["challenges"][j], p, L) for j in range(n)]
+    shifts = [1 << (32 * l) for l in range(L)]
+    py_tables = {}
+    for i, v in enumerate(names):
+        acc = tables[i, 0].tolist()
+        for l in range(1, L):
+            acc = [a + w * shifts[l] for a, w in zip(acc, tables[i, l].tolist())]
+        py_tables[v] = acc
+    del tables
+    t0 = time.perf_counter()
+    claim0, evals = sumcheck_reference(py_tables, q=p, expression=spec.expression, challenges=chals, num_rounds=n)
+    sec = time.perf_counter() - t0
+    got = [[int(x) for x in row] for row in evals]
+    exp = [[from_mont(want["round_polys"][j][t], p, L) for t in range(want["round_polys"].shape[1])]
+           for j in range(n)]
+    return spec.index, sec, bool(got == exp and int(claim0) == from_mont(want["claim0"], p, L))
+
+
+def run_stream(name: str, ref_src: Path) -> dict:
+    import multiprocessing as mp
+
+    sample = stream_sample(name)
+    cores = os.cpu_count() or 1
+    jobs = [(str(ref_src), sp, bw) for sp, bw in sorted(sample, key=lambda x: -x[0].num_vars)]  # longest first
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_stream_worker, jobs, chunksize=1)
+    wall = time.perf_counter() - t0
+    one = sum(sec for _i, sec, _ok in res)
+    sizes = sorted(sp.num_vars for sp, _bw in sample)
+    return {"config": name, "proofs": len(sample), "num_vars": [sizes[0], sizes[-1]],
+            "fields": sorted({bw for _sp, bw in sample}),
+            "reference_py_one_thread_s": round(one, 2), "reference_py_one_thread_proofs_per_s": len(sample) / one,
+            "reference_py_pool_s": round(wall, 2), "reference_py_pool_proofs_per_s": len(sample) / wall,
+            "pool_processes": cores, "host_cpu": cpu_model(), "nproc": cores,
+            "timing": "per proof: sumcheck_reference alone in a pool worker (one thread); pool: wall time of the "
+                      "whole sample including the C oracle's table generation and challenges",
+            "outputs_equal_c_oracle": all(ok for _i, _s, ok in res)}
+
+
 def main() -> int:
     ref = os.environ.get("SUMCHECK_REFERENCE")
     if not ref:
@@ -113,7 +196,7 @@ def main() -> int:
                 "note": "reference.py timed single-threaded where the reference source lives (not the GPU host)"})
     results = doc.setdefault("configs", {})
     for name in names:
-        r = run(name, Path(ref) / "src")
+        r = run_stream(name, Path(ref) / "src") if name in STREAMS else run(name, Path(ref) / "src")
         results[name] = r
         OUT.write_text(json.dumps(doc, indent=1) + "\n")
         print(json.dumps(r), flush=True)
