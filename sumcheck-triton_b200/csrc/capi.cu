@@ -111,7 +111,7 @@ struct ProveRun {
       while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
       smem = static_cast<size_t>(threads) * per_thread;
     } else {
-      smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
+      smem = shape_round_smem_bytes(L, K, shape, threads);  // block_reduce scratch (+ the pair stage)
     }
     int blocks_per_sm = 0;
     SC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, threads, smem));

@@ -203,6 +203,12 @@ template <int L, int K, int D>
 struct SetRoundAttrs {
   static int run() {
     SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+    if constexpr (D == 4) {  // the shape kernels (the 2-limb Goldilocks ones stage pairs in shared memory)
+      SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, 4, kShapeZerocheck>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kMaxDynSmem));
+      SC_CUDA(cudaFuncSetAttribute(round_kernel<L, K, 4, kShapeAbcg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kMaxDynSmem));
+    }
     return SC_OK;
   }
 };

@@ -349,6 +349,36 @@ __device__ __forceinline__ Fe<2> shape_value_lazy(const Fe<2> (&v)[6], const Gol
 #ifndef SC_EARLY_LOADS
 #define SC_EARLY_LOADS 1
 #endif
+
+// 2-limb Goldilocks shape kernels copy each thread's next pair into shared memory with
+// asynchronous copies (cp.async) while the current pair is evaluated, so its loads are in
+// flight during the arithmetic instead of before it. One stage per thread, laid out
+// [table][limb][thread] (16-byte entries in fold rounds, 8-byte in round 0) after the block
+// reduction's scratch; the next pair's copies are issued only after every value of the
+// current stage has been consumed by an arithmetic instruction, and each thread waits for its
+// own copies alone (cp.async.wait_group), so no block barrier is involved.
+#ifndef SC_GOLD_ASYNC
+#define SC_GOLD_ASYNC 1
+#endif
+__host__ __device__ constexpr bool gold_async_stage(int L, int K, int shape) {
+  return SC_GOLD_ASYNC && L == 2 && K == kFieldGoldilocks && shape != kShapeGeneric && SC_GOLD_SHAPE_FMA &&
+         SC_GOLD_LAZY;
+}
+// Dynamic shared memory (bytes) of a compile-time shape round kernel of `threads` threads.
+__host__ __device__ constexpr size_t shape_round_smem_bytes(int L, int K, int shape, int threads) {
+  return 4 * (static_cast<size_t>(threads / 32) * kMaxPoints * L +
+              (gold_async_stage(L, K, shape) ? static_cast<size_t>(threads) * shape_tables(shape) * L * 4 : 0));
+}
+__device__ __forceinline__ void cp_async_16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 #ifndef SC_PAIR_UNROLL
 #define SC_PAIR_UNROLL 1
 #endif
@@ -372,10 +402,64 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
   const int tid = threadIdx.x, nthr = blockDim.x;
   constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
   constexpr bool kGoldLazy = SHAPE != kShapeGeneric && L == 2 && K == kFieldGoldilocksFma && SC_GOLD_LAZY;
+  constexpr bool kAsync = kGoldLazy && SC_GOLD_ASYNC;
   const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
+  // kAsync: this thread's stage, after the block reduction's scratch (16-byte aligned)
+  uint32_t* const stage = sv + (nthr / 32) * kMaxPoints * L;
+  auto issue = [&](uint64_t qn) {  // copies of pair qn into the stage
+#pragma unroll
+    for (int i = 0; i < NR; ++i)
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        const uint32_t* plane = src + (static_cast<uint64_t>(E.role[i]) * L + l) * src_len;
+        const int slot = (i * L + l) * nthr + tid;
+        if (fold)
+          cp_async_16(reinterpret_cast<uint4*>(stage) + slot, reinterpret_cast<const uint4*>(plane) + qn);
+        else
+          cp_async_8(reinterpret_cast<uint2*>(stage) + slot, reinterpret_cast<const uint2*>(plane) + qn);
+      }
+    cp_async_commit();
+  };
+  if constexpr (kAsync) {
+    if (first < last) issue(first);
+  }
 #pragma unroll(SHAPE == kShapeGeneric ? 1 : kPairUnroll)
   for (uint64_t q = first; q < last; q += stride) {
     Fe<L> sh_v[NR], sh_d[NR];
+    if constexpr (kAsync) {
+      cp_async_wait_all();  // this pair's copies (this thread's own) have landed
+      if (fold) {
+        const uint64_t dst_len = src_len >> 1;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+          Fe<L> x0, x1, x2, x3;
+#pragma unroll
+          for (int l = 0; l < L; ++l) {
+            const uint4 v = reinterpret_cast<const uint4*>(stage)[(i * L + l) * nthr + tid];
+            x0.w[l] = v.x; x1.w[l] = v.y; x2.w[l] = v.z; x3.w[l] = v.w;
+          }
+          const Fe<L> e = fe_add(x0, fe_mul(r_prev, fe_sub(x1, x0, F), F), F);
+          const Fe<L> o = fe_add(x2, fe_mul(r_prev, fe_sub(x3, x2, F), F), F);
+#pragma unroll
+          for (int l = 0; l < L; ++l)
+            reinterpret_cast<uint2*>(dst + (static_cast<uint64_t>(E.role[i]) * L + l) * dst_len)[q] = make_uint2(e.w[l], o.w[l]);
+          sh_v[i] = e;
+          sh_d[i] = o;
+        }
+        // every value of the stage has been consumed by the folds: the next pair may land
+        if (q + stride < last) issue(q + stride);
+      } else {
+#pragma unroll
+        for (int i = 0; i < NR; ++i)
+#pragma unroll
+          for (int l = 0; l < L; ++l) {
+            const uint2 v = reinterpret_cast<const uint2*>(stage)[(i * L + l) * nthr + tid];
+            sh_v[i].w[l] = v.x;
+            sh_d[i].w[l] = v.y;
+          }
+        // the next pair is issued after the differences below, which consume every value
+      }
+    } else
 #if SC_EARLY_LOADS
     if constexpr (SHAPE != kShapeGeneric && L <= 2) {
       // every load of the pair first (one 16- or 8-byte load per table and limb plane), then
@@ -467,6 +551,9 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
         const Fe<L> o = sh_d[r];
         sh_d[r] = fe_sub(o, sh_v[r], F);
         sh_v[r] = o;
+      }
+      if constexpr (kAsync) {
+        if (!fold && q + stride < last) issue(q + stride);
       }
       if (!skip1) acc[1] = gl_add(acc[1], shape_value_lazy(sh_v, gk, shape), gk);
 #pragma unroll

@@ -85,7 +85,7 @@ struct SplitSetup {
   static int run(sc_split* S) {
     int threads = kernel_threads(L);
     if (S->E.shape != kShapeGeneric && D == 4) {
-      S->smem = static_cast<size_t>(threads / 32) * kMaxPoints * L * 4;  // block_reduce scratch
+      S->smem = shape_round_smem_bytes(L, K, S->E.shape, threads);  // block_reduce scratch (+ the pair stage)
     } else {
       const int per_thread = round_smem_words_per_thread(S->K, L) * 4;
       while (threads > 32 && threads * per_thread > kMaxDynSmem) threads -= 32;
