@@ -360,14 +360,24 @@ __device__ __forceinline__ Fe<2> shape_value_lazy(const Fe<2> (&v)[6], const Gol
 #ifndef SC_GOLD_ASYNC
 #define SC_GOLD_ASYNC 1
 #endif
+// The same stage for the 8-limb g(abc + de) shape kernel (SC_L8_ASYNC; 96 KB a block of 128
+// threads, 2 blocks an SM) measured slower on B200: plain BLS n = 22 3.37 against 3.25 ms
+// (255 registers with 120 bytes of spills, against none). Off.
+#ifndef SC_L8_ASYNC
+#define SC_L8_ASYNC 0
+#endif
 __host__ __device__ constexpr bool gold_async_stage(int L, int K, int shape) {
   return SC_GOLD_ASYNC && L == 2 && K == kFieldGoldilocks && shape != kShapeGeneric && SC_GOLD_SHAPE_FMA &&
          SC_GOLD_LAZY;
 }
+__host__ __device__ constexpr bool l8_async_stage(int L, int shape) { return SC_L8_ASYNC && L >= 8 && shape == kShapeAbcg; }
+__host__ __device__ constexpr bool shape_async_stage(int L, int K, int shape) {
+  return gold_async_stage(L, K, shape) || l8_async_stage(L, shape);
+}
 // Dynamic shared memory (bytes) of a compile-time shape round kernel of `threads` threads.
 __host__ __device__ constexpr size_t shape_round_smem_bytes(int L, int K, int shape, int threads) {
   return 4 * (static_cast<size_t>(threads / 32) * kMaxPoints * L +
-              (gold_async_stage(L, K, shape) ? static_cast<size_t>(threads) * shape_tables(shape) * L * 4 : 0));
+              (shape_async_stage(L, K, shape) ? static_cast<size_t>(threads) * shape_tables(shape) * L * 4 : 0));
 }
 __device__ __forceinline__ void cp_async_16(void* smem_dst, const void* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -402,7 +412,7 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
   const int tid = threadIdx.x, nthr = blockDim.x;
   constexpr int NR = SHAPE == kShapeGeneric ? 1 : shape_tables(SHAPE);
   constexpr bool kGoldLazy = SHAPE != kShapeGeneric && L == 2 && K == kFieldGoldilocksFma && SC_GOLD_LAZY;
-  constexpr bool kAsync = kGoldLazy && SC_GOLD_ASYNC;
+  constexpr bool kAsync = (kGoldLazy && SC_GOLD_ASYNC) || l8_async_stage(L, SHAPE);
   const int nv = SHAPE == kShapeGeneric ? E.num_vars : NR;
   // kAsync: this thread's stage, after the block reduction's scratch (16-byte aligned)
   uint32_t* const stage = sv + (nthr / 32) * kMaxPoints * L;
@@ -572,6 +582,9 @@ __device__ __forceinline__ void process_pairs(const uint32_t* __restrict__ src, 
         const Fe<L> o = sh_d[r];
         sh_d[r] = fe_sub(o, sh_v[r], F);
         sh_v[r] = o;
+      }
+      if constexpr (kAsync) {
+        if (!fold && q + stride < last) issue(q + stride);
       }
       if (!skip1) acc[1] = fe_add(acc[1], shape_value<L, K>(sh_v, F, std::integral_constant<int, SHAPE>{}), F);
 #pragma unroll
